@@ -1,0 +1,302 @@
+/*
+ * skyweaver_b200.h -- C ABI of the B200-native skyweaver beamforming hot path.
+ *
+ * Conventions
+ *   - Every entry point returns an int status (SW_OK == 0).  On failure the
+ *     message is available from sw_last_error() (thread local).  No C++
+ *     exception crosses this boundary.
+ *   - Pointers named d_* are device pointers (caller allocated unless stated),
+ *     h_* are host pointers.  Sizes are element counts unless named *_bytes.
+ *   - Every kernel entry point is asynchronous on the given stream
+ *     (cudaStream_t passed as sw_stream_t; NULL = legacy default stream).
+ *   - int8 complex voltages are (re, im) byte pairs ("char2").
+ *
+ * Layouts
+ *   TAFTP  [heap][antenna][channel][256 samples][pol][re,im]   (input files)
+ *   FTPA   [channel][sample][pol][antenna][re,im]              (reference stages)
+ *   FPACT  [channel][pol][antenna][re|im][row_stride samples]  (B200 planar,
+ *          stream-major layout used inside the pipeline; sample s of stream
+ *          (f,p,a) lives at byte ((((f*P+p)*A+a)*2+c)*row_stride + offset + s))
+ *   weights FBA   [channel][beam][antenna][re,im]              (reference)
+ *   weights GEMM  [channel][re-row|im-row][beam][antenna][2]   (tensor-core
+ *          A operand: re-row = (w_re, -w_im), im-row = (w_im, w_re))
+ *   CB output TFB [sample/tscrunch][channel][beam] int8
+ *   IB output BTF [beamset][sample/tscrunch][channel] (float raw and int8)
+ *   IDD output TDB [sample][dm][beam] int8
+ *
+ * Each declaration names the reference (erc-compact/skyweaver, paths relative
+ * to the project root) interface it replaces.
+ */
+#ifndef SKYWEAVER_B200_H
+#define SKYWEAVER_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+typedef struct CUstream_st* sw_stream_t;
+
+enum sw_status {
+    SW_OK              = 0,
+    SW_ERR_INVALID     = 1, /* bad argument or size (std::runtime_error in the reference) */
+    SW_ERR_CUDA        = 2, /* CUDA runtime / driver error */
+    SW_ERR_UNSUPPORTED = 3, /* shape outside what the kernels implement */
+    SW_ERR_TIMEOUT     = 4, /* a bounded device-side wait gave up */
+    SW_ERR_STATE       = 5, /* call out of order (e.g. scalings before stats) */
+    SW_ERR_EPOCH       = 6  /* InvalidDelayEpoch (DelayManager.cuh:19-34) */
+};
+
+enum sw_stokes { SW_STOKES_I = 0, SW_STOKES_Q = 1, SW_STOKES_U = 2, SW_STOKES_V = 3 };
+
+/* Library identification and error reporting. */
+int sw_version(void);
+const char* sw_last_error(void);
+/* Device-side error word shared by the kernels with bounded waits
+ * (0 = clean).  sw_reset_device_error clears it. */
+int sw_read_device_error(int* h_code);
+int sw_reset_device_error(void);
+
+/* ------------------------------------------------------------------ */
+/* Transposer                                                           */
+/* ------------------------------------------------------------------ */
+/* Replaces Transposer::transpose (cpp/skyweaver/Transposer.cuh:66-69,
+ * cpp/skyweaver/src/Transposer.cu:117-184): TAFTP -> FTPA with the antenna
+ * dimension zero padded from input_nantennas to output_nantennas. */
+int sw_transpose_ftpa(const void* d_taftp, void* d_ftpa, int nheaps,
+                      int input_nantennas, int output_nantennas, int nchans,
+                      sw_stream_t stream);
+
+/* B200 form of the same stage: TAFTP -> FPACT written at
+ * [sample_offset, sample_offset + nheaps*256) of rows of row_stride samples
+ * (the pipeline keeps coherent-dedispersion history in front of the gulp). */
+int sw_transpose_fpact(const void* d_taftp, void* d_fpact, int nheaps,
+                       int input_nantennas, int output_nantennas, int nchans,
+                       size_t row_stride, size_t sample_offset,
+                       sw_stream_t stream);
+
+/* Layout converters between the reference FTPA layout and FPACT. */
+int sw_ftpa_to_fpact(const void* d_ftpa, void* d_fpact, int nchans,
+                     int nsamples, int nantennas, size_t row_stride,
+                     size_t sample_offset, sw_stream_t stream);
+int sw_fpact_to_ftpa(const void* d_fpact, void* d_ftpa, int nchans,
+                     int nsamples, int nantennas, size_t row_stride,
+                     size_t sample_offset, sw_stream_t stream);
+
+/* Copy the last `history` samples of every FPACT row to its front
+ * (overlap-save history for the next gulp; replaces the per-channel copies of
+ * BufferedDispenser::hoard, cpp/skyweaver/src/BufferedDispenser.cu:29-66). */
+int sw_fpact_keep_history(void* d_fpact, size_t nrows, size_t row_stride,
+                          size_t history, sw_stream_t stream);
+
+/* ------------------------------------------------------------------ */
+/* StatisticsCalculator                                                 */
+/* ------------------------------------------------------------------ */
+/* Replaces StatisticsCalculator::calculate_statistics
+ * (cpp/skyweaver/StatisticsCalculator.cuh:65,
+ *  cpp/skyweaver/src/StatisticsCalculator.cu:54-85,104-130).
+ * Output d_stats: float [nchans][npol][nant][4] = {mean, std, skew, kurtosis}
+ * over the 2*nsamples real and imaginary values of each (f,p,a).
+ * d_scratch: caller-provided device workspace of
+ * sw_statistics_scratch_bytes() bytes (exact int64 moment sums). */
+size_t sw_statistics_scratch_bytes(int nchans, int npol, int nant);
+int sw_statistics(const void* d_fpact, size_t row_stride, size_t sample_offset,
+                  int nchans, int npol, int nant, int nsamples,
+                  void* d_scratch, float* d_stats, sw_stream_t stream);
+
+/* Replaces StatisticsCalculator::update_scalings
+ * (cpp/skyweaver/StatisticsCalculator.cuh:96-97,
+ *  cpp/skyweaver/src/StatisticsCalculator.cu:132-239), computed on the
+ * device.  Outputs are indexed [beamset*nchans + chan] (the reference writes
+ * [chan] for every beamset). */
+int sw_update_scalings(const float* d_stats, const float* d_beamset_weights,
+                       int nbeamsets, int nchans, int npol, int nant,
+                       int cb_tscrunch, int ib_tscrunch, float output_level,
+                       float* d_cb_offsets, float* d_cb_scaling,
+                       float* d_ib_offsets, float* d_ib_scaling,
+                       sw_stream_t stream);
+
+/* ------------------------------------------------------------------ */
+/* WeightsManager                                                       */
+/* ------------------------------------------------------------------ */
+/* Replaces WeightsManager::weights (cpp/skyweaver/WeightsManager.cuh:58-65,
+ * cpp/skyweaver/src/WeightsManager.cu:16-87,109-139).
+ * d_delays: float3 [nbeams][nant] (weight, offset s, rate s/s);
+ * d_freqs: double [nchans] Hz.  Either output may be NULL. */
+int sw_generate_weights(const float* d_delays, const double* d_freqs,
+                        int nant, int nbeams, int nchans, double current_epoch,
+                        double delay_epoch, void* d_weights_fba,
+                        void* d_weights_gemm, sw_stream_t stream);
+/* Reference FBA weights -> GEMM layout (for caller-supplied weights). */
+int sw_pack_weights(const void* d_weights_fba, void* d_weights_gemm,
+                    int nchans, int nbeams, int nant, sw_stream_t stream);
+
+/* ------------------------------------------------------------------ */
+/* IncoherentBeamformer                                                 */
+/* ------------------------------------------------------------------ */
+/* Replaces IncoherentBeamformer<BfTraits>::beamform
+ * (cpp/skyweaver/IncoherentBeamformer.cuh:84-91,
+ *  cpp/skyweaver/src/IncoherentBeamformer.cu:15-91,108-182) for the single
+ * Stokes traits.  Uses the per-beamset antenna weights of the reference's
+ * CPU implementation (IncoherentBeamformerTester.cu:68-70). */
+int sw_incoherent_beamform(const void* d_fpact, size_t row_stride,
+                           size_t sample_offset, int nchans, int nsamples,
+                           int nant, int tscrunch, const float* d_scale,
+                           const float* d_offset,
+                           const float* d_beamset_weights, int nbeamsets,
+                           int stokes, float* d_raw, int8_t* d_out,
+                           sw_stream_t stream);
+
+/* ------------------------------------------------------------------ */
+/* CoherentBeamformer (tcgen05 int8 tensor cores)                       */
+/* ------------------------------------------------------------------ */
+/* One GEMM problem: a coherent DM (voltage block) x a contiguous beam range.
+ * The plain form launches one problem; the grouped form runs all problems
+ * of a gulp in one persistent launch with a ragged work queue. */
+typedef struct sw_cb_problem {
+    const void* d_fpact;   /* dedispersed voltages for this DM (FPACT)   */
+    int8_t* d_out;         /* TFB output for this DM                      */
+    const float* d_ib_raw; /* IB raw power BTF [beamset][T/ts][F] for DM  */
+    int beam_start;        /* first beam of the range                     */
+    int beam_count;        /* beams in the range                          */
+} sw_cb_problem;
+
+typedef struct sw_cb_shape {
+    int nchans;
+    int nsamples;       /* per gulp; multiple of 64                       */
+    int nantennas;      /* 16, 32 or 64                                   */
+    int nbeams;         /* total beams (TFB row length)                   */
+    int tscrunch;       /* 1..32, power of two                            */
+    int stokes;         /* sw_stokes                                      */
+    int ib_subtract;    /* SKYWEAVER_IB_SUBTRACTION (default 1)           */
+    size_t row_stride;  /* FPACT row stride (samples)                     */
+    size_t sample_offset;
+} sw_cb_shape;
+
+/* Replaces CoherentBeamformer<BfTraits>::beamform
+ * (cpp/skyweaver/CoherentBeamformer.cuh:84-92,
+ *  cpp/skyweaver/src/CoherentBeamformer.cu:12-174,191-270).
+ * d_weights_gemm: sw_generate_weights/sw_pack_weights GEMM layout;
+ * d_scale/d_offset: [beamset][chan]; d_mapping: int [nbeams] beam->beamset.
+ * d_debug_voltages: optional int32 [F][T][P][B][2] exact beam voltages
+ * (test hook; NULL in production). */
+int sw_coherent_beamform(const sw_cb_shape* shape, const sw_cb_problem* problem,
+                         const void* d_weights_gemm, const float* d_scale,
+                         const float* d_offset, const int* d_mapping,
+                         int32_t* d_debug_voltages, sw_stream_t stream);
+/* Batched form: all (DM x beam range) problems in one persistent launch. */
+int sw_coherent_beamform_grouped(const sw_cb_shape* shape,
+                                 const sw_cb_problem* h_problems,
+                                 int nproblems, const void* d_weights_gemm,
+                                 const float* d_scale, const float* d_offset,
+                                 const int* d_mapping, sw_stream_t stream);
+
+/* ------------------------------------------------------------------ */
+/* CoherentDedisperser (FP64 chirp, FP32 Stockham-class FFT)            */
+/* ------------------------------------------------------------------ */
+/* Bytes of the device setup block (per-pass FFT twiddle tables followed by
+ * the chirp tables) for sw_cdd_chirps / sw_coherent_dedisperse; 0 if
+ * fft_len is not a supported power of two (256 .. 8192). */
+size_t sw_cdd_setup_bytes(int ndms, int nchans, int fft_len);
+
+/* Replaces create_coherent_dedisperser_config's response tables, i.e.
+ * get_dm_responses / DMResponse
+ * (cpp/skyweaver/src/CoherentDedisperser.cu:61-104,293-359): FP64 chirp
+ * phases stored as complex float [ndms][nchans][fft_len] in the FFT's
+ * internal (digit-reversed) bin order, plus FP64-computed twiddles.
+ * low_freq is the band's lower edge and bw its width (Hz). */
+int sw_cdd_chirps(const float* h_dms, int ndms, int nchans, int fft_len,
+                  double low_freq, double bw, void* d_setup,
+                  sw_stream_t stream);
+
+/* Replaces CoherentDedisperser::dedisperse
+ * (cpp/skyweaver/CoherentDedisperser.cuh:77-80,
+ *  cpp/skyweaver/src/CoherentDedisperser.cu:142-225) for all channels,
+ * antennas, pols and DMs of a gulp with correct overlap-save: input rows
+ * hold `overlap` history samples then nsamples new samples
+ * (row_stride >= overlap + nsamples); output d_out[dm] is FPACT with
+ * row stride out_row_stride holding nsamples samples delayed by overlap/2.
+ * Requantisation wraps to int8 like the reference. */
+int sw_coherent_dedisperse(const void* d_fpact_in, size_t row_stride,
+                           int nchans, int npol, int nant, int nsamples,
+                           int fft_len, int overlap, const void* d_setup,
+                           int ndms, void* const* h_d_out,
+                           size_t out_row_stride, sw_stream_t stream);
+
+/* ------------------------------------------------------------------ */
+/* IncoherentDedisperser                                                */
+/* ------------------------------------------------------------------ */
+/* Replaces IncoherentDedisperser::dedisperse<int8 TFB, int8 TDB>
+ * (cpp/skyweaver/IncoherentDedisperser.cuh:24-26,
+ *  cpp/skyweaver/src/IncoherentDedisperser.cu:66-125) on the GPU.
+ * d_delays: int [ndms][nchans] sample delays; scale_factor as the
+ * reference's prepare() computes it. */
+int sw_incoherent_dedisperse(const int8_t* d_tfb, int nsamples, int nchans,
+                             int nbeams, const int* d_delays, int ndms,
+                             int max_delay, int tscrunch, float scale_factor,
+                             int8_t* d_tdb, sw_stream_t stream);
+
+/* ------------------------------------------------------------------ */
+/* BeamformerPipeline                                                   */
+/* ------------------------------------------------------------------ */
+/* Replaces BeamformerPipeline<CBH,IBH,StatsH,BfTraits>
+ * (cpp/skyweaver/BeamformerPipeline.cuh:48-67,
+ *  cpp/skyweaver/detail/BeamformerPipeline.cu:44-301) with device-buffer
+ * handlers: each gulp's stage chain is one CUDA graph. */
+typedef struct sw_pipeline sw_pipeline;
+
+typedef struct sw_pipeline_config {
+    int nantennas;          /* padded antennas (multiple of 16, <= 64)  */
+    int input_nantennas;    /* antennas present in TAFTP input           */
+    int nchans;
+    int nbeams;
+    int gulp_samples;       /* multiple of 256                           */
+    int tscrunch;           /* CB and IB tscrunch                        */
+    int stokes;
+    int ib_subtract;
+    float output_level;
+    double centre_frequency;
+    double bandwidth;
+    int ndms;               /* coherent DMs                              */
+    const float* dms;       /* host array [ndms]                         */
+    int fft_len;            /* 0 = automatic                             */
+    int enable_coherent_dedispersion;
+    int grouped;            /* 1 = batched persistent CB launch          */
+    int use_graph;          /* 1 = capture the gulp chain as a graph     */
+    int nbeamsets;
+    const float* beamset_weights; /* host [nbeamsets][nantennas]         */
+    const int* beamset_mapping;   /* host [nbeams]                       */
+} sw_pipeline_config;
+
+int sw_pipeline_create(const sw_pipeline_config* cfg, sw_pipeline** out);
+int sw_pipeline_destroy(sw_pipeline* p);
+/* Delay model (host float3 [nbeams][nant]) and its epoch. */
+int sw_pipeline_set_delays(sw_pipeline* p, const float* h_delays,
+                           double delay_epoch);
+/* Run one gulp whose TAFTP input is already on the device. */
+int sw_pipeline_process_device(sw_pipeline* p, const void* d_taftp,
+                               double epoch, sw_stream_t stream);
+/* Run one gulp from pinned host memory: H2D copy, chain, and D2H of the
+ * coherent-beam output of every DM into h_cb_out (may be NULL). */
+int sw_pipeline_process_host(sw_pipeline* p, const void* h_taftp,
+                             double epoch, void* h_cb_out,
+                             sw_stream_t stream);
+/* Device pointers to the last gulp's outputs. */
+int sw_pipeline_outputs(sw_pipeline* p, int dm_idx, const int8_t** d_cb_tfb,
+                        const float** d_ib_raw, const int8_t** d_ib_btf,
+                        const float** d_stats);
+size_t sw_pipeline_cb_bytes_per_dm(const sw_pipeline* p);
+int sw_pipeline_fft_len(const sw_pipeline* p, int* fft_len, int* overlap);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+#ifdef __cplusplus
+}
+#endif
+#endif /* SKYWEAVER_B200_H */

@@ -1,0 +1,427 @@
+// BeamformerPipeline on the B200 (C ABI object behind sw_pipeline_*).
+//
+// Reference: cpp/skyweaver/detail/BeamformerPipeline.cu:44-301.  The
+// reference runs ~10 synchronising stage calls per DM per gulp and 64
+// serial per-channel dedispersion launches; here one gulp is
+//
+//   [epoch H2D] -> weights -> TAFTP->FPACT transpose -> statistics
+//   -> (gulp 0: scalings) -> coherent dedispersion of all channels for all
+//   DMs -> history copy -> incoherent beam per DM
+//   -> one persistent grouped tensor-core launch for all (DM x beamset)
+//
+// all on one stream, captured once as a CUDA graph per input/output buffer
+// pair.  process_host double-buffers the pinned-host input and the outputs
+// so that the H2D of gulp g+1 and the D2H of gulp g-1 overlap the compute
+// of gulp g on separate copy streams.
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <vector>
+
+#include "../sw_common.cuh"
+
+namespace swb {
+int launch_weights(const float* d_delays, const double* d_freqs, int nant, int nbeams,
+                   int nchans, double current_epoch, double delay_epoch,
+                   const double* d_epochs, void* d_fba, void* d_gemm, cudaStream_t stream);
+}
+
+namespace {
+
+constexpr double kDmConst = 4.148806423e15;  // dedispersion_utils.cuh:12-13
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+    int alloc(size_t bytes)
+    {
+        n = bytes;
+        if(bytes == 0) return SW_OK;
+        SW_CUDA_CHECK(cudaMalloc(&p, bytes));
+        return SW_OK;
+    }
+    ~DevBuf()
+    {
+        if(p) cudaFree(p);
+    }
+    template <typename T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+#define SW_TRY(expr)                 \
+    do {                             \
+        int _rc = (expr);            \
+        if(_rc != SW_OK) return _rc; \
+    } while(0)
+
+}  // namespace
+
+struct sw_pipeline {
+    sw_pipeline_config cfg{};
+    std::vector<float> dms;
+    std::vector<float> bw;  // beamset weights [S][A]
+    std::vector<int> mapping;
+    std::vector<double> freqs;
+    int nheaps = 0, T = 0, F = 0, A = 0, B = 0, S = 0, ndm = 0, ts = 0;
+    int fft_len = 0, overlap = 0;  // overlap: multiple of 16
+    size_t ext_stride = 0, ext_off = 0, dd_stride = 0;
+    size_t nrows = 0;  // F * P * A * 2
+
+    DevBuf taftp[2];
+    DevBuf ext;
+    std::vector<DevBuf> dd;
+    DevBuf stats, stats_scratch;
+    DevBuf cb_off, cb_scl, ib_off, ib_scl;
+    DevBuf d_bw, d_map, d_delays, d_freqs, d_wgemm, d_setup;
+    DevBuf epochs;  // [2 parities][2] doubles
+    std::vector<DevBuf> ib_raw[2], ib_i8[2], cb[2];
+    double* h_epochs = nullptr;  // pinned [2][2]
+    double delay_epoch = 0.0;
+    bool have_delays = false;
+
+    cudaStream_t compute = nullptr, h2d = nullptr, d2h = nullptr;
+    cudaEvent_t h2d_done[2]{}, comp_done[2]{}, d2h_done[2]{};
+    bool scalings_done = false;
+    long gulp = 0;
+    int last_par = 0;  // output parity of the last processed gulp
+    std::map<std::pair<const void*, int>, cudaGraphExec_t> graphs;
+
+    ~sw_pipeline()
+    {
+        for(auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+        for(int i = 0; i < 2; ++i) {
+            if(h2d_done[i]) cudaEventDestroy(h2d_done[i]);
+            if(comp_done[i]) cudaEventDestroy(comp_done[i]);
+            if(d2h_done[i]) cudaEventDestroy(d2h_done[i]);
+        }
+        if(compute) cudaStreamDestroy(compute);
+        if(h2d) cudaStreamDestroy(h2d);
+        if(d2h) cudaStreamDestroy(d2h);
+        if(h_epochs) cudaFreeHost(h_epochs);
+    }
+
+    size_t cb_bytes() const { return (size_t)(T / ts) * F * B; }
+    size_t ib_elems() const { return (size_t)S * (T / ts) * F; }
+
+    int init(const sw_pipeline_config& c);
+    int enqueue_chain(const void* d_in, int parity, bool first);
+    int run(const void* d_in, int parity, double epoch);
+};
+
+int sw_pipeline::init(const sw_pipeline_config& c)
+{
+    cfg = c;
+    A = c.nantennas, F = c.nchans, B = c.nbeams, T = c.gulp_samples, ts = c.tscrunch;
+    SW_REQUIRE(A == 16 || A == 32 || A == 64, "pipeline: nantennas must be 16, 32 or 64");
+    SW_REQUIRE(c.input_nantennas > 0 && c.input_nantennas <= A,
+               "Input number of antennas must be <= to the maximum nantennas");
+    SW_REQUIRE(T > 0 && T % 256 == 0, "Gulp size is not a multiple of the number of samples per heap");
+    SW_REQUIRE(F > 0 && B > 0, "pipeline: empty shape");
+    SW_REQUIRE(c.ndms > 0 && c.dms, "No DDPlan set for pipeline");
+    SW_REQUIRE(c.nbeamsets > 0 && c.beamset_weights && c.beamset_mapping,
+               "pipeline: beamset weights and mapping are required");
+    nheaps = T / 256;
+    S      = c.nbeamsets;
+    ndm    = c.ndms;
+    dms.assign(c.dms, c.dms + ndm);
+    bw.assign(c.beamset_weights, c.beamset_weights + (size_t)S * A);
+    mapping.assign(c.beamset_mapping, c.beamset_mapping + B);
+    for(int m : mapping) SW_REQUIRE(m >= 0 && m < S, "pipeline: beamset mapping out of range");
+    // PipelineConfig::calculate_channel_frequencies (PipelineConfig.cpp:188-203)
+    const double chbw = c.bandwidth / F;
+    const double fbottom = c.centre_frequency - c.bandwidth / 2.0;
+    for(int i = 0; i < F; ++i) freqs.push_back(fbottom + chbw / 2.0 + chbw * i);
+
+    // Coherent dedispersion plan: overlap = largest intra-channel DM smear
+    // (lowest channel, largest DM), rounded up to a multiple of 16.
+    if(c.enable_coherent_dedispersion) {
+        const float f_low = (float)(c.centre_frequency - c.bandwidth / 2.0f);
+        const double tsamp = 1.0 / chbw;
+        double maxdm = 0.0;
+        for(float d : dms) maxdm = std::max(maxdm, (double)d);
+        const double f1 = f_low, f2 = f_low + chbw;
+        const double smear = kDmConst * (1.0 / (f1 * f1) - 1.0 / (f2 * f2)) * maxdm;
+        int ov = (int)std::ceil(smear / tsamp);
+        overlap = (ov + 15) / 16 * 16;
+        if(c.fft_len > 0) {
+            fft_len = c.fft_len;
+        } else {
+            double best = 1e30;
+            for(int n = 1024; n <= 8192; n *= 2) {
+                if(n <= overlap) continue;
+                const double cost = std::log2((double)n) / (1.0 - (double)overlap / n);
+                if(cost < best - 1e-9) { best = cost; fft_len = n; }
+            }
+        }
+        SW_REQUIRE(fft_len > overlap && fft_len >= 256 && fft_len <= 8192,
+                   "pipeline: DM smear of %d samples needs an FFT longer than 8192", overlap);
+        SW_REQUIRE(T >= overlap, "pipeline: gulp shorter than the dedispersion overlap");
+    } else {
+        overlap = 0;
+        fft_len = 0;
+    }
+    ext_off    = (size_t)overlap;
+    ext_stride = (size_t)overlap + T;
+    dd_stride  = (size_t)T;
+    nrows      = (size_t)F * 2 * A * 2;
+
+    SW_CUDA_CHECK(cudaStreamCreateWithFlags(&compute, cudaStreamNonBlocking));
+    SW_CUDA_CHECK(cudaStreamCreateWithFlags(&h2d, cudaStreamNonBlocking));
+    SW_CUDA_CHECK(cudaStreamCreateWithFlags(&d2h, cudaStreamNonBlocking));
+    for(int i = 0; i < 2; ++i) {
+        SW_CUDA_CHECK(cudaEventCreateWithFlags(&h2d_done[i], cudaEventDisableTiming));
+        SW_CUDA_CHECK(cudaEventCreateWithFlags(&comp_done[i], cudaEventDisableTiming));
+        SW_CUDA_CHECK(cudaEventCreateWithFlags(&d2h_done[i], cudaEventDisableTiming));
+    }
+    SW_CUDA_CHECK(cudaMallocHost(&h_epochs, 4 * sizeof(double)));
+    memset(h_epochs, 0, 4 * sizeof(double));
+
+    const size_t taftp_bytes = (size_t)nheaps * c.input_nantennas * F * 256 * 2 * 2;
+    SW_TRY(taftp[0].alloc(taftp_bytes));
+    SW_TRY(taftp[1].alloc(taftp_bytes));
+    SW_TRY(ext.alloc(nrows * ext_stride));
+    SW_CUDA_CHECK(cudaMemset(ext.p, 0, ext.n));  // zero history for gulp 0
+    if(c.enable_coherent_dedispersion) {
+        dd.resize(ndm);
+        for(int d = 0; d < ndm; ++d) SW_TRY(dd[d].alloc(nrows * dd_stride));
+        SW_TRY(d_setup.alloc(sw_cdd_setup_bytes(ndm, F, fft_len)));
+        const double low = (double)(float)(c.centre_frequency - c.bandwidth / 2.0f);
+        SW_TRY(sw_cdd_chirps(dms.data(), ndm, F, fft_len, low, c.bandwidth, d_setup.p,
+                             (sw_stream_t)compute));
+    }
+    SW_TRY(stats.alloc((size_t)F * 2 * A * 4 * sizeof(float)));
+    SW_TRY(stats_scratch.alloc(sw_statistics_scratch_bytes(F, 2, A)));
+    for(DevBuf* b : {&cb_off, &cb_scl, &ib_off, &ib_scl}) SW_TRY(b->alloc((size_t)S * F * sizeof(float)));
+    SW_TRY(d_bw.alloc(bw.size() * sizeof(float)));
+    SW_TRY(d_map.alloc(mapping.size() * sizeof(int)));
+    SW_TRY(d_delays.alloc((size_t)B * A * 3 * sizeof(float)));
+    SW_TRY(d_freqs.alloc(freqs.size() * sizeof(double)));
+    SW_TRY(d_wgemm.alloc((size_t)F * 2 * B * 2 * A));
+    SW_TRY(epochs.alloc(4 * sizeof(double)));
+    SW_CUDA_CHECK(cudaMemcpy(d_bw.p, bw.data(), d_bw.n, cudaMemcpyHostToDevice));
+    SW_CUDA_CHECK(cudaMemcpy(d_map.p, mapping.data(), d_map.n, cudaMemcpyHostToDevice));
+    SW_CUDA_CHECK(cudaMemcpy(d_freqs.p, freqs.data(), d_freqs.n, cudaMemcpyHostToDevice));
+    SW_CUDA_CHECK(cudaMemset(d_delays.p, 0, d_delays.n));
+    for(int par = 0; par < 2; ++par) {
+        ib_raw[par].resize(ndm);
+        ib_i8[par].resize(ndm);
+        cb[par].resize(ndm);
+        for(int d = 0; d < ndm; ++d) {
+            SW_TRY(ib_raw[par][d].alloc(ib_elems() * sizeof(float)));
+            SW_TRY(ib_i8[par][d].alloc(ib_elems()));
+            SW_TRY(cb[par][d].alloc(cb_bytes()));
+        }
+    }
+    SW_CUDA_CHECK(cudaStreamSynchronize(compute));
+    return SW_OK;
+}
+
+// One gulp's device chain on `compute` (captured into a graph when enabled).
+int sw_pipeline::enqueue_chain(const void* d_in, int parity, bool first)
+{
+    cudaStream_t s = compute;
+    sw_stream_t ss = (sw_stream_t)s;
+    double* d_ep = epochs.as<double>() + 2 * parity;
+    SW_CUDA_CHECK(cudaMemcpyAsync(d_ep, h_epochs + 2 * parity, 2 * sizeof(double),
+                                  cudaMemcpyHostToDevice, s));
+    SW_TRY(swb::launch_weights(d_delays.as<float>(), d_freqs.as<double>(), A, B, F, 0.0, 0.0,
+                               d_ep, nullptr, d_wgemm.p, s));
+    SW_TRY(sw_transpose_fpact(d_in, ext.p, nheaps, cfg.input_nantennas, A, F, ext_stride,
+                              ext_off, ss));
+    SW_TRY(sw_statistics(ext.p, ext_stride, ext_off, F, 2, A, T, stats_scratch.p,
+                         stats.as<float>(), ss));
+    if(first) {
+        SW_TRY(sw_update_scalings(stats.as<float>(), d_bw.as<float>(), S, F, 2, A, ts, ts,
+                                  cfg.output_level, cb_off.as<float>(), cb_scl.as<float>(),
+                                  ib_off.as<float>(), ib_scl.as<float>(), ss));
+    }
+    std::vector<const void*> volt(ndm);
+    size_t vstride = ext_stride, voff = ext_off;
+    if(cfg.enable_coherent_dedispersion) {
+        std::vector<void*> outs(ndm);
+        for(int d = 0; d < ndm; ++d) outs[d] = dd[d].p;
+        SW_TRY(sw_coherent_dedisperse(ext.p, ext_stride, F, 2, A, T, fft_len, overlap,
+                                      d_setup.p, ndm, outs.data(), dd_stride, ss));
+        SW_TRY(sw_fpact_keep_history(ext.p, nrows, ext_stride, (size_t)overlap, ss));
+        for(int d = 0; d < ndm; ++d) volt[d] = dd[d].p;
+        vstride = dd_stride;
+        voff = 0;
+    } else {
+        for(int d = 0; d < ndm; ++d) volt[d] = ext.p;
+    }
+    for(int d = 0; d < ndm; ++d) {
+        SW_TRY(sw_incoherent_beamform(volt[d], vstride, voff, F, T, A, ts, ib_scl.as<float>(),
+                                      ib_off.as<float>(), d_bw.as<float>(), S, cfg.stokes,
+                                      ib_raw[parity][d].as<float>(),
+                                      ib_i8[parity][d].as<int8_t>(), ss));
+    }
+    sw_cb_shape shape{F, T, A, B, ts, cfg.stokes, cfg.ib_subtract, vstride, voff};
+    // problems: one per (DM, contiguous run of beams in the same beamset)
+    std::vector<sw_cb_problem> probs;
+    for(int d = 0; d < ndm; ++d) {
+        int b = 0;
+        while(b < B) {
+            int e = b + 1;
+            while(e < B && mapping[e] == mapping[b]) ++e;
+            probs.push_back({volt[d], cb[parity][d].as<int8_t>(), ib_raw[parity][d].as<float>(),
+                             b, e - b});
+            b = e;
+        }
+    }
+    if(probs.size() > 96) {  // too ragged for one launch table: one range per DM
+        probs.clear();
+        for(int d = 0; d < ndm; ++d)
+            probs.push_back({volt[d], cb[parity][d].as<int8_t>(), ib_raw[parity][d].as<float>(), 0, B});
+    }
+    if(cfg.grouped) {
+        SW_TRY(sw_coherent_beamform_grouped(&shape, probs.data(), (int)probs.size(), d_wgemm.p,
+                                            cb_scl.as<float>(), cb_off.as<float>(),
+                                            d_map.as<int>(), ss));
+    } else {
+        for(auto& pr : probs)
+            SW_TRY(sw_coherent_beamform(&shape, &pr, d_wgemm.p, cb_scl.as<float>(),
+                                        cb_off.as<float>(), d_map.as<int>(), nullptr, ss));
+    }
+    return SW_OK;
+}
+
+int sw_pipeline::run(const void* d_in, int parity, double epoch)
+{
+    SW_REQUIRE(have_delays, "pipeline: no delay model set (sw_pipeline_set_delays)");
+    last_par = parity;
+    h_epochs[2 * parity + 0] = epoch;
+    h_epochs[2 * parity + 1] = delay_epoch;
+    if(!scalings_done || !cfg.use_graph) {
+        SW_TRY(enqueue_chain(d_in, parity, !scalings_done));
+        scalings_done = true;
+        return SW_OK;
+    }
+    auto key = std::make_pair(d_in, parity);
+    auto it = graphs.find(key);
+    if(it == graphs.end()) {
+        cudaGraph_t g;
+        SW_CUDA_CHECK(cudaStreamBeginCapture(compute, cudaStreamCaptureModeThreadLocal));
+        int rc = enqueue_chain(d_in, parity, false);
+        cudaError_t e = cudaStreamEndCapture(compute, &g);
+        if(rc != SW_OK) return rc;
+        SW_CUDA_CHECK(e);
+        cudaGraphExec_t ge;
+        SW_CUDA_CHECK(cudaGraphInstantiate(&ge, g, 0));
+        cudaGraphDestroy(g);
+        it = graphs.emplace(key, ge).first;
+    }
+    SW_CUDA_CHECK(cudaGraphLaunch(it->second, compute));
+    return SW_OK;
+}
+
+using namespace swb;
+
+extern "C" {
+
+int sw_pipeline_create(const sw_pipeline_config* cfg, sw_pipeline** out)
+{
+    SW_REQUIRE(cfg && out, "sw_pipeline_create: null argument");
+    *out = nullptr;
+    sw_pipeline* p = new sw_pipeline();
+    int rc = p->init(*cfg);
+    if(rc != SW_OK) {
+        delete p;
+        return rc;
+    }
+    *out = p;
+    return SW_OK;
+}
+
+int sw_pipeline_destroy(sw_pipeline* p)
+{
+    if(p) {
+        cudaStreamSynchronize(p->compute);
+        cudaStreamSynchronize(p->h2d);
+        cudaStreamSynchronize(p->d2h);
+        delete p;
+    }
+    return SW_OK;
+}
+
+int sw_pipeline_set_delays(sw_pipeline* p, const float* h_delays, double delay_epoch)
+{
+    SW_REQUIRE(p && h_delays, "sw_pipeline_set_delays: null argument");
+    SW_CUDA_CHECK(cudaStreamSynchronize(p->compute));
+    SW_CUDA_CHECK(cudaMemcpy(p->d_delays.p, h_delays, p->d_delays.n, cudaMemcpyHostToDevice));
+    p->delay_epoch = delay_epoch;
+    p->have_delays = true;
+    return SW_OK;
+}
+
+int sw_pipeline_process_device(sw_pipeline* p, const void* d_taftp, double epoch,
+                               sw_stream_t stream)
+{
+    SW_REQUIRE(p && d_taftp, "sw_pipeline_process_device: null argument");
+    cudaStream_t s = as_cuda(stream);
+    // order after the caller's stream, run, and make the caller's stream wait
+    SW_CUDA_CHECK(cudaEventRecord(p->h2d_done[0], s));
+    SW_CUDA_CHECK(cudaStreamWaitEvent(p->compute, p->h2d_done[0], 0));
+    SW_CUDA_CHECK(cudaStreamWaitEvent(p->compute, p->d2h_done[0], 0));
+    int rc = p->run(d_taftp, 0, epoch);
+    if(rc != SW_OK) return rc;
+    SW_CUDA_CHECK(cudaEventRecord(p->comp_done[0], p->compute));
+    SW_CUDA_CHECK(cudaStreamWaitEvent(s, p->comp_done[0], 0));
+    ++p->gulp;
+    return SW_OK;
+}
+
+int sw_pipeline_process_host(sw_pipeline* p, const void* h_taftp, double epoch, void* h_cb_out,
+                             sw_stream_t stream)
+{
+    SW_REQUIRE(p && h_taftp, "sw_pipeline_process_host: null argument");
+    const int par = (int)(p->gulp & 1);
+    // H2D into this parity's input buffer once its previous gulp consumed it
+    SW_CUDA_CHECK(cudaStreamWaitEvent(p->h2d, p->comp_done[par], 0));
+    SW_CUDA_CHECK(cudaMemcpyAsync(p->taftp[par].p, h_taftp, p->taftp[par].n,
+                                  cudaMemcpyHostToDevice, p->h2d));
+    SW_CUDA_CHECK(cudaEventRecord(p->h2d_done[par], p->h2d));
+    SW_CUDA_CHECK(cudaStreamWaitEvent(p->compute, p->h2d_done[par], 0));
+    SW_CUDA_CHECK(cudaStreamWaitEvent(p->compute, p->d2h_done[par], 0));
+    int rc = p->run(p->taftp[par].p, par, epoch);
+    if(rc != SW_OK) return rc;
+    SW_CUDA_CHECK(cudaEventRecord(p->comp_done[par], p->compute));
+    SW_CUDA_CHECK(cudaStreamWaitEvent(p->d2h, p->comp_done[par], 0));
+    if(h_cb_out) {
+        const size_t nb = p->cb_bytes();
+        for(int d = 0; d < p->ndm; ++d)
+            SW_CUDA_CHECK(cudaMemcpyAsync(static_cast<uint8_t*>(h_cb_out) + d * nb,
+                                          p->cb[par][d].p, nb, cudaMemcpyDeviceToHost, p->d2h));
+    }
+    SW_CUDA_CHECK(cudaEventRecord(p->d2h_done[par], p->d2h));
+    SW_CUDA_CHECK(cudaStreamWaitEvent(as_cuda(stream), p->d2h_done[par], 0));
+    ++p->gulp;
+    return SW_OK;
+}
+
+int sw_pipeline_outputs(sw_pipeline* p, int dm_idx, const int8_t** d_cb_tfb,
+                        const float** d_ib_raw, const int8_t** d_ib_btf, const float** d_stats)
+{
+    SW_REQUIRE(p && dm_idx >= 0 && dm_idx < p->ndm, "sw_pipeline_outputs: bad arguments");
+    const int par = p->last_par;
+    if(d_cb_tfb) *d_cb_tfb = p->cb[par][dm_idx].as<int8_t>();
+    if(d_ib_raw) *d_ib_raw = p->ib_raw[par][dm_idx].as<float>();
+    if(d_ib_btf) *d_ib_btf = p->ib_i8[par][dm_idx].as<int8_t>();
+    if(d_stats) *d_stats = p->stats.as<float>();
+    return SW_OK;
+}
+
+size_t sw_pipeline_cb_bytes_per_dm(const sw_pipeline* p) { return p ? p->cb_bytes() : 0; }
+
+int sw_pipeline_fft_len(const sw_pipeline* p, int* fft_len, int* overlap)
+{
+    SW_REQUIRE(p, "sw_pipeline_fft_len: null pipeline");
+    if(fft_len) *fft_len = p->fft_len;
+    if(overlap) *overlap = p->overlap;
+    return SW_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,609 @@
+// CoherentBeamformer on the B200: tcgen05 int8 tensor-core GEMM with a fused
+// detection / tscrunch / IB-subtraction / quantisation epilogue.
+//
+// Reference: cpp/skyweaver/src/CoherentBeamformer.cu:12-174 (dp4a on CUDA
+// cores) and its CPU form cpp/skyweaver/test/src/CoherentBeamformerTester.cu
+// :43-152.
+//
+// Formulation (per channel f):
+//   A  (M = 128 beams x K = 2*nant int8, K-major, SMEM via TMA):
+//        re block rows (w_re, -w_im) per antenna, im block rows (w_im, w_re)
+//   B  (N = 2 pols x 64 samples, K = (antenna, re|im), MN-major): the planar
+//        FPACT voltage rows, one TMA box [2 pols][2*nant rows][64 samples]
+//   D_re = A_re . B, D_im = A_im . B  (int32 in TMEM, exact)
+// so TMEM lane b holds Re and Im of beam b for both pols and all 64 samples
+// of the tile and the whole Stokes / tscrunch reduction is thread local.
+// The epilogue repeats the reference's float operations in the reference's
+// order with IEEE single rounding, so the int8 output is bit-identical to
+// the CPU implementation.
+//
+// Roles (one CTA per SM, persistent over a ragged work queue):
+//   warp 0      TMA producer (weights double buffered, voltages 4 stages)
+//   warp 1      TMEM allocator + single-thread MMA issuer
+//   warps 2..9  epilogue (two warps per TMEM lane quarter)
+// TMEM: 512 columns = 2 accumulator buffers x (D_re 128 | D_im 128).
+// Every wait is bounded by a kernel-wide deadline; on expiry the CTA records
+// DEV_ERR_CB_TIMEOUT in the device error word, stops issuing work and exits cleanly.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
+#include "sw_common.cuh"
+
+namespace swb {
+namespace cb {
+
+constexpr int kM           = 128;  // beams per tile
+constexpr int kTileT       = 64;   // samples per tile
+constexpr int kN           = 2 * kTileT;
+constexpr int kVStages     = 4;
+constexpr int kWStages     = 2;
+constexpr int kTilesPerItem = 16;  // 1024 samples of one channel per item
+constexpr int kMaxDm       = 16;
+constexpr int kMaxProblems = 96;
+constexpr int kEpiWarps    = 8;
+constexpr int kThreads     = 32 * (2 + kEpiWarps);
+constexpr int kTmemCols    = 512;
+
+struct Problem {
+    int8_t* out;
+    const float* ib_raw;
+    int dm;
+    int beam_start;
+    int beam_count;
+    int item_start;
+};
+
+struct Params {
+    CUtensorMap vmap[kMaxDm];
+    CUtensorMap wmap;
+    Problem prob[kMaxProblems];
+    int nproblems, nitems;
+    int nchans, nsamples, nant, nbeams, tscrunch, stokes, ib_subtract;
+    int kbytes, ntc;
+    size_t sample_offset;
+    const float* scale;
+    const float* offset;
+    const int* mapping;
+    int32_t* debug;
+    int* err;
+    uint32_t idesc;
+    uint32_t w_layout, w_sbo16, v_lbo16;
+    unsigned long long timeout_ns;
+};
+
+// ------------------------------------------------------------ PTX helpers
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ unsigned long long globaltimer()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait: false if the kernel-wide deadline passed or another role
+// already aborted.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
+                                          volatile int* abort_flag,
+                                          unsigned long long deadline, int* err)
+{
+    uint32_t n = 0;
+    while(!mbar_try_wait(bar, parity)) {
+        if(*abort_flag) return false;
+        if((++n & 1023u) == 0 && globaltimer() > deadline) {
+            *abort_flag = 1;
+            if(err) atomicExch(err, DEV_ERR_CB_TIMEOUT);
+            return false;
+        }
+    }
+    return true;
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map,
+                                            uint64_t* bar, int x, int y)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+        "[%0], [%1, {%3, %4}], [%2];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map,
+                                            uint64_t* bar, int x, int y, int z)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+        "[%0], [%1, {%3, %4, %5}], [%2];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z)
+        : "memory");
+}
+
+// tcgen05 shared-memory matrix descriptor (sm_100 "version 1" format).
+__device__ __forceinline__ uint64_t make_desc(uint32_t saddr, uint32_t lbo16,
+                                              uint32_t sbo16, uint32_t layout)
+{
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)(lbo16 & 0x3FFFu) << 16;
+    d |= (uint64_t)(sbo16 & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)(layout & 7u) << 61;
+    return d;
+}
+
+__device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t adesc,
+                                       uint64_t bdesc, uint32_t idesc,
+                                       uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar)
+{
+    asm volatile(
+        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+            smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+#define SW_TMEM_LD16(taddr, r)                                                             \
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 "                                 \
+                 "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"        \
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), \
+                   "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]),            \
+                   "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])         \
+                 : "r"(taddr))
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// Stokes from the exact beam voltages, reference op order (beamformer_utils.cuh:125-140)
+__device__ __forceinline__ float stokes_f(int stokes, float r0, float i0, float r1, float i1)
+{
+    switch(stokes) {
+    case 0: return fadd(fadd(fmul(r0, r0), fmul(i0, i0)), fadd(fmul(r1, r1), fmul(i1, i1)));
+    case 1: return fsub(fadd(fmul(r0, r0), fmul(i0, i0)), fadd(fmul(r1, r1), fmul(i1, i1)));
+    case 2: return fmul(2.0f, fsub(fmul(r0, r1), fmul(i0, -i1)));
+    default: return fmul(2.0f, fadd(fmul(r0, -i1), fmul(i0, r1)));
+    }
+}
+
+struct Item {
+    int p, f, tc, b0;
+};
+
+__device__ __forceinline__ Item decode(const Params& P, int item)
+{
+    int p = 0;
+    while(p + 1 < P.nproblems && P.prob[p + 1].item_start <= item) ++p;
+    const Problem& pr = P.prob[p];
+    const int nblk  = (pr.beam_count + kM - 1) / kM;
+    const int local = item - pr.item_start;
+    Item it;
+    it.p  = p;
+    const int mb = local % nblk;
+    const int rest = local / nblk;
+    it.tc = rest % P.ntc;
+    it.f  = rest / P.ntc;
+    it.b0 = pr.beam_start + mb * kM;
+    return it;
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+cb_kernel(const __grid_constant__ Params P)
+{
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    // 1024-byte aligned carve-up
+    uint8_t* base = reinterpret_cast<uint8_t*>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const int wtile = kM * P.kbytes;              // one A block
+    const int vtile = 2 * P.kbytes * kTileT;       // one B stage
+    uint8_t* wbuf = base;                          // [kWStages][2][wtile]
+    uint8_t* vbuf = wbuf + kWStages * 2 * wtile;   // [kVStages][vtile]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(vbuf + kVStages * vtile);
+    uint64_t* v_full    = bars;
+    uint64_t* v_empty   = v_full + kVStages;
+    uint64_t* w_full    = v_empty + kVStages;
+    uint64_t* w_empty   = w_full + kWStages;
+    uint64_t* acc_full  = w_empty + kWStages;
+    uint64_t* acc_empty = acc_full + 2;
+    uint32_t* s_tmem    = reinterpret_cast<uint32_t*>(acc_empty + 2);
+    volatile int* s_abort = reinterpret_cast<volatile int*>(s_tmem + 1);
+
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const unsigned long long deadline = globaltimer() + P.timeout_ns;
+
+    if(threadIdx.x == 0) {
+        for(int i = 0; i < kVStages; ++i) { mbar_init(&v_full[i], 1); mbar_init(&v_empty[i], 1); }
+        for(int i = 0; i < kWStages; ++i) { mbar_init(&w_full[i], 1); mbar_init(&w_empty[i], 1); }
+        for(int i = 0; i < 2; ++i) { mbar_init(&acc_full[i], 1); mbar_init(&acc_empty[i], kEpiWarps); }
+        *s_abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if(warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(s_tmem)),
+                     "r"(kTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = *s_tmem;
+    const int ntiles_gulp = P.nsamples / kTileT;
+
+    if(warp == 0) {
+        if(lane == 0) {
+            // ---------------------------------------------------- producer
+            int vs = 0, ws = 0;
+            uint32_t vph = 0, wph = 0;
+            for(int item = blockIdx.x; item < P.nitems && !*s_abort; item += gridDim.x) {
+                const Item it = decode(P, item);
+                const Problem& pr = P.prob[it.p];
+                if(!mbar_wait(&w_empty[ws], wph ^ 1, s_abort, deadline, P.err)) break;
+                mbar_expect_tx(&w_full[ws], 2 * wtile);
+                uint8_t* wdst = wbuf + ws * 2 * wtile;
+                tma_load_2d(wdst, &P.wmap, &w_full[ws], 0, (it.f * 2 + 0) * P.nbeams + it.b0);
+                tma_load_2d(wdst + wtile, &P.wmap, &w_full[ws], 0, (it.f * 2 + 1) * P.nbeams + it.b0);
+                if(++ws == kWStages) { ws = 0; wph ^= 1; }
+                const int tile0 = it.tc * kTilesPerItem;
+                const int tile1 = min(ntiles_gulp, tile0 + kTilesPerItem);
+                for(int tile = tile0; tile < tile1; ++tile) {
+                    if(!mbar_wait(&v_empty[vs], vph ^ 1, s_abort, deadline, P.err)) break;
+                    mbar_expect_tx(&v_full[vs], vtile);
+                    tma_load_3d(vbuf + vs * vtile, &P.vmap[pr.dm], &v_full[vs],
+                                (int)(P.sample_offset + (size_t)tile * kTileT), 0, it.f * 2);
+                    if(++vs == kVStages) { vs = 0; vph ^= 1; }
+                }
+            }
+        }
+    } else if(warp == 1) {
+        if(lane == 0) {
+            // ------------------------------------------------- MMA issuer
+            int vs = 0, ws = 0, ab = 0;
+            uint32_t vph = 0, wph = 0, aph = 0;
+            const int ksteps = P.kbytes / 32;
+            for(int item = blockIdx.x; item < P.nitems && !*s_abort; item += gridDim.x) {
+                const Item it = decode(P, item);
+                if(!mbar_wait(&w_full[ws], wph, s_abort, deadline, P.err)) break;
+                const uint32_t wa = smem_u32(wbuf + ws * 2 * wtile);
+                const int tile0 = it.tc * kTilesPerItem;
+                const int tile1 = min(ntiles_gulp, tile0 + kTilesPerItem);
+                bool ok = true;
+                for(int tile = tile0; tile < tile1; ++tile) {
+                    if(!mbar_wait(&v_full[vs], vph, s_abort, deadline, P.err)) { ok = false; break; }
+                    if(!mbar_wait(&acc_empty[ab], aph ^ 1, s_abort, deadline, P.err)) { ok = false; break; }
+                    fence_after();
+                    const uint32_t vb = smem_u32(vbuf + vs * vtile);
+                    const uint32_t d_re = tmem + ab * 256;
+                    const uint32_t d_im = d_re + 128;
+                    for(int ks = 0; ks < ksteps; ++ks) {
+                        const uint64_t adr = make_desc(wa + ks * 32, 1, P.w_sbo16, P.w_layout);
+                        const uint64_t adi = make_desc(wa + wtile + ks * 32, 1, P.w_sbo16, P.w_layout);
+                        const uint64_t bd  = make_desc(vb + ks * 2048, P.v_lbo16, 32, 4 /*SW64*/);
+                        mma_i8(d_re, adr, bd, P.idesc, ks > 0);
+                        mma_i8(d_im, adi, bd, P.idesc, ks > 0);
+                    }
+                    mma_commit(&v_empty[vs]);
+                    mma_commit(&acc_full[ab]);
+                    if(++vs == kVStages) { vs = 0; vph ^= 1; }
+                    if(++ab == 2) { ab = 0; aph ^= 1; }
+                }
+                mma_commit(&w_empty[ws]);
+                if(++ws == kWStages) { ws = 0; wph ^= 1; }
+                if(!ok) break;
+            }
+        }
+    } else {
+        // ------------------------------------------------------ epilogue
+        const int q = warp & 3;          // TMEM lane quarter of this warp
+        const int h = (warp - 2) >> 2;   // which half of the tile's samples
+        const int F = P.nchans;
+        const int nout = P.nsamples / P.tscrunch;
+        int ab = 0;
+        uint32_t aph = 0;
+        for(int item = blockIdx.x; item < P.nitems && !*s_abort; item += gridDim.x) {
+            const Item it = decode(P, item);
+            const Problem& pr = P.prob[it.p];
+            const int b = it.b0 + q * 32 + lane;
+            const bool valid = (b < pr.beam_start + pr.beam_count) && (b < P.nbeams);
+            const int bs = valid ? P.mapping[b] : 0;
+            const float scale = P.scale[bs * F + it.f];
+            const float offs  = P.offset[bs * F + it.f];
+            const int tile0 = it.tc * kTilesPerItem;
+            const int tile1 = min(ntiles_gulp, tile0 + kTilesPerItem);
+            bool ok = true;
+            for(int tile = tile0; tile < tile1; ++tile) {
+                if(!mbar_wait(&acc_full[ab], aph, s_abort, deadline, P.err)) { ok = false; break; }
+                fence_after();
+                float power = 0.0f;
+                int count = 0;
+                for(int g = 0; g < 2; ++g) {
+                    const int col = ab * 256 + h * 32 + g * 16;
+                    const uint32_t ta = tmem + ((uint32_t)(q * 32) << 16) + col;
+                    uint32_t r0[16], r1[16], i0[16], i1[16];
+                    SW_TMEM_LD16(ta, r0);
+                    SW_TMEM_LD16(ta + 64, r1);
+                    SW_TMEM_LD16(ta + 128, i0);
+                    SW_TMEM_LD16(ta + 192, i1);
+                    tmem_wait_ld();
+                    const int tbase = tile * kTileT + h * 32 + g * 16;
+#pragma unroll
+                    for(int t = 0; t < 16; ++t) {
+                        const float fr0 = __int2float_rn((int)r0[t]);
+                        const float fi0 = __int2float_rn((int)i0[t]);
+                        const float fr1 = __int2float_rn((int)r1[t]);
+                        const float fi1 = __int2float_rn((int)i1[t]);
+                        if(P.debug && valid) {
+                            const size_t base_t = (size_t)it.f * P.nsamples + tbase + t;
+                            int2* dbg = reinterpret_cast<int2*>(P.debug);
+                            dbg[(base_t * 2 + 0) * P.nbeams + b] = make_int2((int)r0[t], (int)i0[t]);
+                            dbg[(base_t * 2 + 1) * P.nbeams + b] = make_int2((int)r1[t], (int)i1[t]);
+                        }
+                        power = fadd(power, stokes_f(P.stokes, fr0, fi0, fr1, fi1));
+                        if(++count == P.tscrunch) {
+                            const int to = (tbase + t) / P.tscrunch;
+                            float v;
+                            if(P.ib_subtract) {
+                                const float ib = pr.ib_raw[((size_t)bs * nout + to) * F + it.f];
+                                v = rintf(fdiv(fsub(power, fmul(ib, 16129.0f)), scale));
+                            } else if(P.stokes == 0) {
+                                v = rintf(fdiv(fsub(power, offs), scale));
+                            } else {
+                                v = rintf(fdiv(power, scale));
+                            }
+                            if(valid) pr.out[((size_t)to * F + it.f) * P.nbeams + b] = clamp_i8(v);
+                            power = 0.0f;
+                            count = 0;
+                        }
+                    }
+                }
+                fence_before();
+                __syncwarp();
+                if(lane == 0) mbar_arrive(&acc_empty[ab]);
+                if(++ab == 2) { ab = 0; aph ^= 1; }
+            }
+            if(!ok) break;
+        }
+    }
+    fence_before();
+    __syncthreads();
+    if(warp == 1) {
+        fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(kTmemCols));
+    }
+}
+
+// ------------------------------------------------------------ host side
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+               cudaSuccess &&
+           q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+int make_vmap(CUtensorMap* map, const void* fpact, const sw_cb_shape& s)
+{
+    auto fn = encode_fn();
+    SW_REQUIRE(fn != nullptr, "cuTensorMapEncodeTiled is unavailable");
+    const cuuint64_t dims[3]    = {(cuuint64_t)s.row_stride, (cuuint64_t)(2 * s.nantennas),
+                                   (cuuint64_t)(2 * s.nchans)};
+    const cuuint64_t strides[2] = {(cuuint64_t)s.row_stride,
+                                   (cuuint64_t)(2 * s.nantennas) * s.row_stride};
+    const cuuint32_t box[3]     = {(cuuint32_t)kTileT, (cuuint32_t)(2 * s.nantennas), 2};
+    const cuuint32_t es[3]      = {1, 1, 1};
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void*>(fpact), dims,
+                    strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if(r != CUDA_SUCCESS) {
+        set_error("cuTensorMapEncodeTiled (voltages) failed: %d", (int)r);
+        return SW_ERR_CUDA;
+    }
+    return SW_OK;
+}
+
+int make_wmap(CUtensorMap* map, const void* w, const sw_cb_shape& s)
+{
+    auto fn = encode_fn();
+    SW_REQUIRE(fn != nullptr, "cuTensorMapEncodeTiled is unavailable");
+    const int kb = 2 * s.nantennas;
+    const cuuint64_t dims[2]    = {(cuuint64_t)kb, (cuuint64_t)(2 * s.nchans) * s.nbeams};
+    const cuuint64_t strides[1] = {(cuuint64_t)kb};
+    const cuuint32_t box[2]     = {(cuuint32_t)kb, (cuuint32_t)kM};
+    const cuuint32_t es[2]      = {1, 1};
+    const CUtensorMapSwizzle sw = kb == 128 ? CU_TENSOR_MAP_SWIZZLE_128B
+                                : kb == 64  ? CU_TENSOR_MAP_SWIZZLE_64B
+                                            : CU_TENSOR_MAP_SWIZZLE_32B;
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void*>(w), dims, strides,
+                    box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, sw,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if(r != CUDA_SUCCESS) {
+        set_error("cuTensorMapEncodeTiled (weights) failed: %d", (int)r);
+        return SW_ERR_CUDA;
+    }
+    return SW_OK;
+}
+
+size_t smem_bytes(int kbytes)
+{
+    return 1024 + (size_t)kWStages * 2 * kM * kbytes + (size_t)kVStages * 2 * kbytes * kTileT +
+           (2 * kVStages + 2 * kWStages + 4) * 8 + 16;
+}
+
+int num_sms()
+{
+    static int n = 0;
+    if(n == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if(n <= 0) n = 148;
+    }
+    return n;
+}
+
+int launch(const sw_cb_shape* s, const sw_cb_problem* probs, int nprob,
+           const void* w, const float* scale, const float* offset,
+           const int* mapping, int32_t* debug, cudaStream_t stream)
+{
+    SW_REQUIRE(s && probs && nprob > 0 && w && scale && offset && mapping,
+               "CoherentBeamformer: null argument");
+    SW_REQUIRE(nprob <= kMaxProblems, "CoherentBeamformer: at most %d problems", kMaxProblems);
+    SW_REQUIRE(s->nantennas == 16 || s->nantennas == 32 || s->nantennas == 64,
+               "CoherentBeamformer: nantennas must be 16, 32 or 64 (got %d)", s->nantennas);
+    SW_REQUIRE(s->nsamples > 0 && s->nsamples % kTileT == 0,
+               "Number of samples must be a multiple of %d", kTileT);
+    SW_REQUIRE(s->tscrunch >= 1 && s->tscrunch <= 32 && (s->tscrunch & (s->tscrunch - 1)) == 0,
+               "CoherentBeamformer: tscrunch must be a power of two <= 32");
+    SW_REQUIRE(s->stokes >= 0 && s->stokes <= 3, "CoherentBeamformer: bad Stokes mode");
+    SW_REQUIRE(s->row_stride % 16 == 0 && s->sample_offset % 16 == 0,
+               "CoherentBeamformer: FPACT stride/offset must be multiples of 16");
+    SW_REQUIRE(s->sample_offset + (size_t)s->nsamples <= s->row_stride,
+               "CoherentBeamformer: rows shorter than the gulp");
+    SW_REQUIRE(s->nbeams > 0 && s->nchans > 0, "CoherentBeamformer: empty shape");
+    SW_REQUIRE(s->row_stride <= 0x7fffffffULL, "CoherentBeamformer: row stride too large");
+
+    static thread_local Params P;  // ~6 KB, kept off the stack
+    memset(&P, 0, sizeof(P));
+    const void* dms[kMaxDm];
+    int ndm = 0, item = 0;
+    const int ntc = cdiv(s->nsamples / kTileT, kTilesPerItem);
+    for(int i = 0; i < nprob; ++i) {
+        const sw_cb_problem& pr = probs[i];
+        SW_REQUIRE(pr.d_fpact && pr.d_out && (pr.d_ib_raw || !s->ib_subtract),
+                   "CoherentBeamformer: problem %d has a null pointer", i);
+        SW_REQUIRE(pr.beam_start >= 0 && pr.beam_count > 0 &&
+                       pr.beam_start + pr.beam_count <= s->nbeams,
+                   "CoherentBeamformer: problem %d beam range out of bounds", i);
+        int d = 0;
+        while(d < ndm && dms[d] != pr.d_fpact) ++d;
+        if(d == ndm) {
+            SW_REQUIRE(ndm < kMaxDm, "CoherentBeamformer: at most %d voltage blocks", kMaxDm);
+            dms[ndm] = pr.d_fpact;
+            int rc = make_vmap(&P.vmap[ndm], pr.d_fpact, *s);
+            if(rc) return rc;
+            ++ndm;
+        }
+        P.prob[i].out        = pr.d_out;
+        P.prob[i].ib_raw     = pr.d_ib_raw;
+        P.prob[i].dm         = d;
+        P.prob[i].beam_start = pr.beam_start;
+        P.prob[i].beam_count = pr.beam_count;
+        P.prob[i].item_start = item;
+        item += s->nchans * ntc * cdiv(pr.beam_count, kM);
+    }
+    int rc = make_wmap(&P.wmap, w, *s);
+    if(rc) return rc;
+    P.nproblems   = nprob;
+    P.nitems      = item;
+    P.nchans      = s->nchans;
+    P.nsamples    = s->nsamples;
+    P.nant        = s->nantennas;
+    P.nbeams      = s->nbeams;
+    P.tscrunch    = s->tscrunch;
+    P.stokes      = s->stokes;
+    P.ib_subtract = s->ib_subtract;
+    P.kbytes      = 2 * s->nantennas;
+    P.ntc         = ntc;
+    P.sample_offset = s->sample_offset;
+    P.scale   = scale;
+    P.offset  = offset;
+    P.mapping = mapping;
+    P.debug   = debug;
+    P.err     = device_error_ptr();
+    // kind::i8 instruction descriptor: D=S32, A=B=S8, A K-major, B MN-major,
+    // N=128 (bits 17-22: N>>3), M=128 (bits 24-28: M>>4)
+    P.idesc = (2u << 4) | (1u << 7) | (1u << 10) | (0u << 15) | (1u << 16) |
+              ((uint32_t)(kN >> 3) << 17) | ((uint32_t)(kM >> 4) << 24);
+    P.w_layout = P.kbytes == 128 ? 2u : P.kbytes == 64 ? 4u : 6u;  // SW128/SW64/SW32
+    P.w_sbo16  = (uint32_t)(8 * P.kbytes / 16);                       // 8-row group stride
+    P.v_lbo16  = (uint32_t)(2 * s->nantennas * kTileT / 16);          // pol plane stride
+    P.timeout_ns = 5ull * 1000 * 1000 * 1000;                         // 5 s
+
+    const size_t smem = smem_bytes(P.kbytes);
+    SW_CUDA_CHECK(cudaFuncSetAttribute(cb_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
+    const int grid = P.nitems < num_sms() ? P.nitems : num_sms();
+    cb_kernel<<<grid, kThreads, smem, stream>>>(P);
+    SW_LAUNCH_CHECK();
+    return SW_OK;
+}
+
+}  // namespace cb
+}  // namespace swb
+
+extern "C" {
+
+int sw_coherent_beamform(const sw_cb_shape* shape, const sw_cb_problem* problem,
+                         const void* d_weights_gemm, const float* d_scale,
+                         const float* d_offset, const int* d_mapping,
+                         int32_t* d_debug_voltages, sw_stream_t stream)
+{
+    return swb::cb::launch(shape, problem, 1, d_weights_gemm, d_scale, d_offset, d_mapping,
+                           d_debug_voltages, swb::as_cuda(stream));
+}
+
+int sw_coherent_beamform_grouped(const sw_cb_shape* shape,
+                                 const sw_cb_problem* h_problems, int nproblems,
+                                 const void* d_weights_gemm, const float* d_scale,
+                                 const float* d_offset, const int* d_mapping,
+                                 sw_stream_t stream)
+{
+    return swb::cb::launch(shape, h_problems, nproblems, d_weights_gemm, d_scale, d_offset,
+                           d_mapping, nullptr, swb::as_cuda(stream));
+}
+
+}  // extern "C"

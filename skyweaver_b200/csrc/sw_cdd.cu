@@ -1,0 +1,533 @@
+// CoherentDedisperser on the B200.
+//
+// Reference: cpp/skyweaver/src/CoherentDedisperser.cu:142-225 (per channel:
+// int8 -> complex64, cuFFT forward, chirp multiply, cuFFT inverse, trim
+// overlap/2 each side, /N, round, int8 wrap) with the chirp of
+// DMResponse (:293-336) and the golden-vector generator
+// python/skyweaver_test_utils/dedisperse.py:58-80,143-173.
+//
+// B200 design: one CTA transforms one overlap-save segment of one
+// (channel, pol, antenna) stream entirely in shared memory and registers:
+//   * the forward FFT is an in-place mixed-radix decimation-in-frequency
+//     FFT (first pass radix 2/4/8/16 read straight from the planar int8
+//     rows, then radix-16 passes); its last pass leaves each thread's 16
+//     spectral bins in registers, in digit-reversed order;
+//   * for every coherent DM the thread multiplies those bins by the chirp
+//     (FP64 phases, stored as complex float in the same digit-reversed
+//     order), runs the exact inverse passes (decimation in time, conjugate
+//     twiddles) and the last pass writes the trimmed, scaled, rounded and
+//     int8-wrapped samples straight to the planar output rows.
+// So the forward transform is done once per segment for all DMs, there is
+// no spectrum in HBM, and all global traffic is coalesced byte rows.
+// Twiddles come from per-pass tables (FP64-computed) staged in shared
+// memory; FFT arithmetic is FP32.
+#include "sw_common.cuh"
+
+namespace swb {
+namespace cdd {
+
+constexpr int kMaxDms = 64;
+
+// ---------------------------------------------------------------- plan
+struct Plan {
+    int logn, n, r0, npass;
+    int radix[8];
+    int span[8];    // G_p
+    int stride[8];  // s_p = G_p / R_p
+    int tw_off[8];  // offset (complex entries) of pass p's table
+    int tw_total;
+};
+
+__host__ __device__ constexpr Plan make_plan(int logn)
+{
+    Plan P{};
+    P.logn = logn;
+    P.n    = 1 << logn;
+    const int rem = logn % 4;
+    P.r0 = rem ? (1 << rem) : 16;
+    int g = P.n, off = 0, p = 0;
+    int r = P.r0;
+    while(g > 1) {
+        P.radix[p]  = r;
+        P.span[p]   = g;
+        P.stride[p] = g / r;
+        P.tw_off[p] = off;
+        if(P.stride[p] > 1) off += (r - 1) * P.stride[p];
+        g /= r;
+        r = 16;
+        ++p;
+    }
+    P.npass    = p;
+    P.tw_total = off;
+    return P;
+}
+
+// DIF output position -> natural frequency bin
+__host__ __device__ inline int digit_reverse(const Plan& P, int pos)
+{
+    int k = 0, mult = 1;
+    for(int p = 0; p < P.npass; ++p) {
+        const int q = (pos / P.stride[p]) % P.radix[p];
+        k += q * mult;
+        mult *= P.radix[p];
+    }
+    return k;
+}
+
+// ------------------------------------------------------- complex helpers
+struct c32 {
+    float x, y;
+};
+__device__ __forceinline__ c32 cadd(c32 a, c32 b) { return {a.x + b.x, a.y + b.y}; }
+__device__ __forceinline__ c32 csub(c32 a, c32 b) { return {a.x - b.x, a.y - b.y}; }
+__device__ __forceinline__ c32 cmul(c32 a, c32 b)
+{
+    return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
+}
+__device__ __forceinline__ c32 cmulc(c32 a, c32 b)  // a * conj(b)
+{
+    return {a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y};
+}
+// multiply by -i (forward) or +i (inverse)
+template <bool INV>
+__device__ __forceinline__ c32 rot90(c32 a)
+{
+    return INV ? c32{-a.y, a.x} : c32{a.y, -a.x};
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft2(c32* x)
+{
+    c32 a = x[0], b = x[1];
+    x[0] = cadd(a, b);
+    x[1] = csub(a, b);
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft4(c32& x0, c32& x1, c32& x2, c32& x3)
+{
+    const c32 t0 = cadd(x0, x2), t1 = csub(x0, x2);
+    const c32 t2 = cadd(x1, x3), t3 = rot90<INV>(csub(x1, x3));
+    x0 = cadd(t0, t2);
+    x2 = csub(t0, t2);
+    x1 = cadd(t1, t3);
+    x3 = csub(t1, t3);
+}
+
+// W_16^k for k = 0..9 (forward sign); constants rounded once by the compiler
+__device__ __forceinline__ c32 w16(int k)
+{
+    const float c1 = 0.92387953251128675613f, s1 = 0.38268343236508977173f;
+    const float c2 = 0.70710678118654752440f;
+    switch(k) {
+    case 0: return {1.0f, 0.0f};
+    case 1: return {c1, -s1};
+    case 2: return {c2, -c2};
+    case 3: return {s1, -c1};
+    case 4: return {0.0f, -1.0f};
+    case 5: return {-s1, -c1};
+    case 6: return {-c2, -c2};
+    case 7: return {-c1, -s1};
+    case 8: return {-1.0f, 0.0f};
+    default: return {-c1, s1};  // k == 9
+    }
+}
+
+// In-register DFT of size 16, natural order in and out.
+template <bool INV>
+__device__ __forceinline__ void dft16(c32* x)
+{
+#pragma unroll
+    for(int r2 = 0; r2 < 4; ++r2) dft4<INV>(x[r2], x[4 + r2], x[8 + r2], x[12 + r2]);
+    // now x[4*q1 + r2] holds A[r2][q1]; twiddle by W16^(r2*q1)
+#pragma unroll
+    for(int r2 = 1; r2 < 4; ++r2)
+#pragma unroll
+        for(int q1 = 1; q1 < 4; ++q1) {
+            c32 w = w16(r2 * q1);
+            if(INV) w.y = -w.y;
+            x[4 * q1 + r2] = cmul(x[4 * q1 + r2], w);
+        }
+#pragma unroll
+    for(int q1 = 0; q1 < 4; ++q1) dft4<INV>(x[4 * q1], x[4 * q1 + 1], x[4 * q1 + 2], x[4 * q1 + 3]);
+    // x[4*q1 + q2] holds X[q1 + 4*q2]; transpose to natural order
+    c32 t[16];
+#pragma unroll
+    for(int q1 = 0; q1 < 4; ++q1)
+#pragma unroll
+        for(int q2 = 0; q2 < 4; ++q2) t[q1 + 4 * q2] = x[4 * q1 + q2];
+#pragma unroll
+    for(int i = 0; i < 16; ++i) x[i] = t[i];
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft8(c32* x)
+{
+    // radix 2 x 4: r = 4*r1 + r2, q = q1 + 2*q2
+#pragma unroll
+    for(int r2 = 0; r2 < 4; ++r2) {
+        c32 a = x[r2], b = x[4 + r2];
+        x[r2] = cadd(a, b);
+        x[4 + r2] = csub(a, b);
+    }
+    // twiddle W8^(r2*q1) on the q1 = 1 half
+    const float c2 = 0.70710678118654752440f;
+    x[5] = cmul(x[5], c32{c2, INV ? c2 : -c2});
+    x[6] = rot90<INV>(x[6]);
+    x[7] = cmul(x[7], c32{-c2, INV ? c2 : -c2});
+    dft4<INV>(x[0], x[1], x[2], x[3]);
+    dft4<INV>(x[4], x[5], x[6], x[7]);
+    c32 t[8];
+#pragma unroll
+    for(int q2 = 0; q2 < 4; ++q2) {
+        t[2 * q2]     = x[q2];
+        t[2 * q2 + 1] = x[4 + q2];
+    }
+#pragma unroll
+    for(int i = 0; i < 8; ++i) x[i] = t[i];
+}
+
+template <int R, bool INV>
+__device__ __forceinline__ void dft(c32* x)
+{
+    if constexpr(R == 16) dft16<INV>(x);
+    else if constexpr(R == 8) dft8<INV>(x);
+    else if constexpr(R == 4) dft4<INV>(x[0], x[1], x[2], x[3]);
+    else dft2<INV>(x);
+}
+
+// one padding slot per 16 complex values keeps the strided radix-16 passes
+// free of shared-memory bank conflicts
+__host__ __device__ constexpr int pad(int i) { return i + (i >> 4); }
+
+struct Args {
+    const uint8_t* in;
+    size_t row_stride;
+    int nstreams;      // F * P * A
+    int nsamples;      // T
+    int overlap;       // O (even)
+    int nseg;
+    int ndms;
+    const c32* tw;     // twiddle tables
+    const c32* chirp;  // [ndms][F][N] digit-reversed
+    int npa;           // P * A (streams per channel)
+    uint8_t* out[kMaxDms];
+    size_t out_stride;
+};
+
+// One radix-R pass of the inverse (DIT) on shared memory.
+template <int LOGN, int R>
+__device__ __forceinline__ void inv_pass(c32* buf, const c32* tw_s, int G, int s,
+                                         int tw_off)
+{
+    constexpr int N   = 1 << LOGN;
+    constexpr int NT  = N / 16;
+    constexpr int BPT = 16 / R;  // butterflies per thread
+#pragma unroll
+    for(int u = 0; u < BPT; ++u) {
+        const int beta = threadIdx.x + u * NT;
+        const int g = beta / s, j = beta - g * s;
+        const int base = g * G + j;
+        c32 z[R];
+#pragma unroll
+        for(int q = 0; q < R; ++q) z[q] = buf[pad(base + q * s)];
+        if(s > 1) {
+#pragma unroll
+            for(int q = 1; q < R; ++q) z[q] = cmulc(z[q], tw_s[tw_off + (q - 1) * s + j]);
+        }
+        dft<R, true>(z);
+#pragma unroll
+        for(int r = 0; r < R; ++r) buf[pad(base + r * s)] = z[r];
+    }
+}
+
+template <int LOGN, int R>
+__device__ __forceinline__ void fwd_pass(c32* buf, const c32* tw_s, int G, int s,
+                                         int tw_off)
+{
+    constexpr int N   = 1 << LOGN;
+    constexpr int NT  = N / 16;
+    constexpr int BPT = 16 / R;
+#pragma unroll
+    for(int u = 0; u < BPT; ++u) {
+        const int beta = threadIdx.x + u * NT;
+        const int g = beta / s, j = beta - g * s;
+        const int base = g * G + j;
+        c32 x[R];
+#pragma unroll
+        for(int r = 0; r < R; ++r) x[r] = buf[pad(base + r * s)];
+        dft<R, false>(x);
+        if(s > 1) {
+#pragma unroll
+            for(int q = 1; q < R; ++q) x[q] = cmul(x[q], tw_s[tw_off + (q - 1) * s + j]);
+        }
+#pragma unroll
+        for(int q = 0; q < R; ++q) buf[pad(base + q * s)] = x[q];
+    }
+}
+
+template <int LOGN>
+__global__ void __launch_bounds__((1 << LOGN) / 16)
+cdd_kernel(const __grid_constant__ Args A)
+{
+    constexpr int N  = 1 << LOGN;
+    constexpr int NT = N / 16;
+    constexpr Plan P = make_plan(LOGN);
+    constexpr int R0 = P.r0;
+    constexpr int B0 = 16 / R0;  // first-pass butterflies per thread
+    extern __shared__ __align__(16) uint8_t smem[];
+    c32* buf  = reinterpret_cast<c32*>(smem);
+    c32* tw_s = buf + pad(N) + 16;
+    for(int i = threadIdx.x; i < P.tw_total; i += NT) tw_s[i] = A.tw[i];
+    __syncthreads();
+
+    const int L = N - A.overlap;
+    const int half = A.overlap / 2;
+    const float inv_n = 1.0f / (float)N;  // exact (power of two)
+    const int nitems = A.nstreams * A.nseg;
+    for(int item = blockIdx.x; item < nitems; item += gridDim.x) {
+        const int stream = item / A.nseg;
+        const int seg    = item - stream * A.nseg;
+        const int f      = stream / A.npa;
+        const uint8_t* row_re = A.in + (size_t)stream * 2 * A.row_stride;
+        const uint8_t* row_im = row_re + A.row_stride;
+        const int start = seg * L;                 // first input sample of the window
+        const int avail = A.overlap + A.nsamples;  // history + gulp
+
+        // ---- forward pass 0 (radix R0, span N) straight from global int8
+        {
+            constexpr int s0 = N / R0;
+#pragma unroll
+            for(int u = 0; u < B0; ++u) {
+                const int j = threadIdx.x + u * NT;
+                c32 x[R0];
+#pragma unroll
+                for(int r = 0; r < R0; ++r) {
+                    const int idx = start + j + r * s0;
+                    x[r] = idx < avail ? c32{(float)(int8_t)row_re[idx], (float)(int8_t)row_im[idx]}
+                                       : c32{0.0f, 0.0f};
+                }
+                dft<R0, false>(x);
+#pragma unroll
+                for(int q = 1; q < R0; ++q) x[q] = cmul(x[q], tw_s[P.tw_off[0] + (q - 1) * s0 + j]);
+#pragma unroll
+                for(int q = 0; q < R0; ++q) buf[pad(j + q * s0)] = x[q];
+            }
+        }
+        __syncthreads();
+        // ---- forward radix-16 passes except the last
+#pragma unroll
+        for(int p = 1; p < P.npass - 1; ++p) {
+            fwd_pass<LOGN, 16>(buf, tw_s, P.span[p], P.stride[p], P.tw_off[p]);
+            __syncthreads();
+        }
+        // ---- last forward pass (span 16, no twiddles): spectrum -> registers
+        c32 spec[16];
+#pragma unroll
+        for(int r = 0; r < 16; ++r) spec[r] = buf[pad(threadIdx.x * 16 + r)];
+        dft16<false>(spec);
+        __syncthreads();
+
+        for(int d = 0; d < A.ndms; ++d) {
+            const c32* ch = A.chirp + ((size_t)d * (A.nstreams / A.npa) + f) * N + threadIdx.x * 16;
+            c32 y[16];
+#pragma unroll
+            for(int q = 0; q < 16; ++q) y[q] = cmul(spec[q], ch[q]);
+            dft16<true>(y);
+#pragma unroll
+            for(int r = 0; r < 16; ++r) buf[pad(threadIdx.x * 16 + r)] = y[r];
+            __syncthreads();
+#pragma unroll
+            for(int p = P.npass - 2; p >= 1; --p) {
+                inv_pass<LOGN, 16>(buf, tw_s, P.span[p], P.stride[p], P.tw_off[p]);
+                __syncthreads();
+            }
+            // ---- inverse pass 0 (radix R0, span N): natural-order output
+            uint8_t* o_re = A.out[d] + (size_t)stream * 2 * A.out_stride;
+            uint8_t* o_im = o_re + A.out_stride;
+            constexpr int s0 = N / R0;
+#pragma unroll
+            for(int u = 0; u < B0; ++u) {
+                const int j = threadIdx.x + u * NT;
+                c32 z[R0];
+#pragma unroll
+                for(int q = 0; q < R0; ++q) z[q] = buf[pad(j + q * s0)];
+#pragma unroll
+                for(int q = 1; q < R0; ++q) z[q] = cmulc(z[q], tw_s[P.tw_off[0] + (q - 1) * s0 + j]);
+                dft<R0, true>(z);
+#pragma unroll
+                for(int r = 0; r < R0; ++r) {
+                    const int i = j + r * s0;           // index within the window
+                    const int m = start + i - half;     // output sample in the gulp
+                    if(i >= half && i < half + L && m < A.nsamples) {
+                        const int vr = __float2int_rn(z[r].x * inv_n);
+                        const int vi = __float2int_rn(z[r].y * inv_n);
+                        o_re[m] = (uint8_t)vr;  // int8 wrap, like static_cast<char>
+                        o_im[m] = (uint8_t)vi;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// ------------------------------------------------------------- setup
+struct SetupArgs {
+    int logn, ndms, nchans;
+    double low_freq, coarse_bw, fine_bw;
+    double prefactor[kMaxDms];
+};
+
+__global__ void twiddle_k(c32* tw, int logn)
+{
+    const Plan P = make_plan(logn);
+    for(int p = 0; p < P.npass; ++p) {
+        const int s = P.stride[p], R = P.radix[p], G = P.span[p];
+        if(s <= 1) continue;
+        for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < (R - 1) * s;
+            i += gridDim.x * blockDim.x) {
+            const int q = i / s + 1, j = i % s;
+            double sn, cs;
+            // exp(-2 pi i j q / G) in FP64
+            sincospi(-2.0 * (double)(j * q) / (double)G, &sn, &cs);
+            tw[P.tw_off[p] + i] = c32{(float)cs, (float)sn};
+        }
+    }
+}
+
+// DMResponse (CoherentDedisperser.cu:313-335) in FP64, stored at the
+// digit-reversed position of its bin.
+__global__ void chirp_k(c32* chirp, SetupArgs S)
+{
+    const Plan P = make_plan(S.logn);
+    const size_t total = (size_t)S.ndms * S.nchans * P.n;
+    for(size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total;
+        i += (size_t)gridDim.x * blockDim.x) {
+        const int pos = (int)(i % P.n);
+        const int c   = (int)((i / P.n) % S.nchans);
+        const int d   = (int)(i / ((size_t)P.n * S.nchans));
+        const int k   = digit_reverse(P, pos);
+        const double nu0   = S.low_freq + c * S.coarse_bw - 0.5 * S.coarse_bw;
+        const double nu    = k * S.fine_bw;
+        const double phase = (nu * nu * S.prefactor[d]) / ((nu0 + nu) * nu0 * nu0);
+        double sn, cs;
+        sincos(phase, &sn, &cs);
+        chirp[i] = c32{(float)cs, (float)sn};
+    }
+}
+
+template <int LOGN>
+int launch_logn(const Args& a, cudaStream_t stream)
+{
+    constexpr int N = 1 << LOGN;
+    constexpr Plan P = make_plan(LOGN);
+    const size_t smem = (size_t)(pad(N) + 16 + P.tw_total) * sizeof(c32);
+    SW_CUDA_CHECK(cudaFuncSetAttribute(cdd_kernel<LOGN>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int dev = 0, nsm = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    SW_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cdd_kernel<LOGN>,
+                                                                 N / 16, smem));
+    if(per_sm < 1) per_sm = 1;
+    const long items = (long)a.nstreams * a.nseg;
+    const long grid  = items < (long)nsm * per_sm ? items : (long)nsm * per_sm;
+    cdd_kernel<LOGN><<<(int)grid, N / 16, smem, stream>>>(a);
+    SW_LAUNCH_CHECK();
+    return SW_OK;
+}
+
+int log2_exact(int n)
+{
+    int l = 0;
+    while((1 << l) < n) ++l;
+    return (1 << l) == n ? l : -1;
+}
+
+}  // namespace cdd
+}  // namespace swb
+
+using namespace swb;
+using namespace swb::cdd;
+
+extern "C" {
+
+size_t sw_cdd_setup_bytes(int ndms, int nchans, int fft_len)
+{
+    const int logn = log2_exact(fft_len);
+    if(logn < 0) return 0;
+    const Plan P = make_plan(logn);
+    return ((size_t)P.tw_total + 16 + (size_t)ndms * nchans * fft_len) * sizeof(c32);
+}
+
+int sw_cdd_chirps(const float* h_dms, int ndms, int nchans, int fft_len,
+                  double low_freq, double bw, void* d_setup, sw_stream_t stream)
+{
+    const int logn = log2_exact(fft_len);
+    SW_REQUIRE(logn >= 8 && logn <= 13, "coherent dedispersion: fft_len must be a power of two in [256, 8192]");
+    SW_REQUIRE(h_dms && ndms > 0 && ndms <= kMaxDms, "coherent dedispersion: 1..%d DMs", kMaxDms);
+    SW_REQUIRE(d_setup && nchans > 0, "coherent dedispersion: bad setup arguments");
+    const Plan P = make_plan(logn);
+    c32* tw = static_cast<c32*>(d_setup);
+    c32* ch = tw + P.tw_total + 16;  // keep the chirp table 128-byte aligned-ish
+    twiddle_k<<<64, 256, 0, as_cuda(stream)>>>(tw, logn);
+    SW_LAUNCH_CHECK();
+    SetupArgs S{};
+    S.logn      = logn;
+    S.ndms      = ndms;
+    S.nchans    = nchans;
+    S.low_freq  = low_freq;
+    S.coarse_bw = bw / nchans;
+    S.fine_bw   = S.coarse_bw / fft_len;
+    for(int d = 0; d < ndms; ++d)
+        S.prefactor[d] = -1.0 * (2.0 * 3.1415926535897932385) * 4.148806423e15 * (double)h_dms[d];
+    chirp_k<<<148 * 4, 256, 0, as_cuda(stream)>>>(ch, S);
+    SW_LAUNCH_CHECK();
+    return SW_OK;
+}
+
+int sw_coherent_dedisperse(const void* d_fpact_in, size_t row_stride,
+                           int nchans, int npol, int nant, int nsamples,
+                           int fft_len, int overlap, const void* d_setup,
+                           int ndms, void* const* h_d_out,
+                           size_t out_row_stride, sw_stream_t stream)
+{
+    const int logn = log2_exact(fft_len);
+    SW_REQUIRE(logn >= 8 && logn <= 13, "coherent dedispersion: fft_len must be a power of two in [256, 8192]");
+    SW_REQUIRE(d_fpact_in && d_setup && h_d_out, "coherent dedispersion: null pointer");
+    SW_REQUIRE(ndms > 0 && ndms <= kMaxDms, "coherent dedispersion: 1..%d DMs", kMaxDms);
+    SW_REQUIRE(overlap >= 0 && overlap % 2 == 0 && overlap < fft_len,
+               "coherent dedispersion: overlap must be even and smaller than the FFT");
+    SW_REQUIRE(nsamples > 0 && (size_t)overlap + nsamples <= row_stride,
+               "coherent dedispersion: input rows must hold history + gulp");
+    SW_REQUIRE((size_t)nsamples <= out_row_stride, "coherent dedispersion: output rows too short");
+    const Plan P = make_plan(logn);
+    Args a{};
+    a.in         = static_cast<const uint8_t*>(d_fpact_in);
+    a.row_stride = row_stride;
+    a.npa        = npol * nant;
+    a.nstreams   = nchans * npol * nant;
+    a.nsamples   = nsamples;
+    a.overlap    = overlap;
+    a.nseg       = cdiv(nsamples, fft_len - overlap);
+    a.ndms       = ndms;
+    a.tw         = static_cast<const c32*>(d_setup);
+    a.chirp      = a.tw + P.tw_total + 16;
+    for(int d = 0; d < ndms; ++d) {
+        SW_REQUIRE(h_d_out[d], "coherent dedispersion: null output for DM %d", d);
+        a.out[d] = static_cast<uint8_t*>(h_d_out[d]);
+    }
+    a.out_stride = out_row_stride;
+    cudaStream_t s = as_cuda(stream);
+    switch(logn) {
+    case 8: return launch_logn<8>(a, s);
+    case 9: return launch_logn<9>(a, s);
+    case 10: return launch_logn<10>(a, s);
+    case 11: return launch_logn<11>(a, s);
+    case 12: return launch_logn<12>(a, s);
+    default: return launch_logn<13>(a, s);
+    }
+}
+
+}  // extern "C"

@@ -1,0 +1,193 @@
+// IncoherentBeamformer on the B200
+// (cpp/skyweaver/src/IncoherentBeamformer.cu:15-91; CPU form
+//  cpp/skyweaver/test/src/IncoherentBeamformerTester.cu:41-103).
+//
+// P[s,t',f] = sum_{t in t'} sum_a w[s,a] * Stokes(v_p0, v_p1)  (float, in the
+// reference's (t outer, a inner) order), then int8 = clamp(rint(rescale)).
+//
+// Every Stokes term of int8 voltages is an exact integer, so when the
+// antenna weights are integers the float chain is exact as long as the sum
+// of |terms| stays below 2^24.  The kernel therefore sums the terms with
+// dp4a in integers, checks that bound, and only walks the float chain in the
+// reference order (slow path) for outputs that fail it.  The result is
+// bit-identical to the reference's CPU implementation in both cases.
+//
+// One thread per (channel, output sample); the planar FPACT rows make each
+// thread's tscrunch samples a contiguous 4/8/16-byte load, coalesced across
+// the warp.  The kernel is HBM bound (one read of the voltages).
+#include "sw_common.cuh"
+
+namespace swb {
+namespace {
+
+constexpr int kMaxBs = 8;          // beamsets per pass (registers)
+constexpr int kMaxAnt = 256;
+
+struct IbArgs {
+    const uint8_t* fpact;
+    size_t row_stride, offset;
+    int nchans, nsamples, nant, tscrunch, nbeamsets, stokes;
+    const float *scale, *offset_v, *weights;
+    float* raw;
+    int8_t* out;
+};
+
+__device__ __forceinline__ float stokes_f(int stokes, float r0, float i0,
+                                          float r1, float i1)
+{
+    // beamformer_utils.cuh:125-140 with the reference's op order
+    switch(stokes) {
+    case 0: return fadd(fadd(fmul(r0, r0), fmul(i0, i0)), fadd(fmul(r1, r1), fmul(i1, i1)));
+    case 1: return fsub(fadd(fmul(r0, r0), fmul(i0, i0)), fadd(fmul(r1, r1), fmul(i1, i1)));
+    case 2: return fmul(2.0f, fsub(fmul(r0, r1), fmul(i0, -i1)));
+    default: return fmul(2.0f, fadd(fmul(r0, -i1), fmul(i0, r1)));
+    }
+}
+
+__global__ void __launch_bounds__(128)
+ib_k(IbArgs args, int bs0)
+{
+    __shared__ float sw[kMaxBs][kMaxAnt];
+    __shared__ int s_intw[kMaxBs];
+    const int nbs = min(kMaxBs, args.nbeamsets - bs0);
+    for(int i = threadIdx.x; i < kMaxBs * args.nant; i += blockDim.x) {
+        const int s = i / args.nant, a = i % args.nant;
+        sw[s][a] = (s < nbs) ? args.weights[(size_t)(bs0 + s) * args.nant + a] : 0.0f;
+    }
+    __syncthreads();
+    if(threadIdx.x < kMaxBs) {
+        int ok = 1;
+        for(int a = 0; a < args.nant; ++a) {
+            const float w = sw[threadIdx.x][a];
+            ok &= (w == rintf(w)) && fabsf(w) <= 1024.0f;
+        }
+        s_intw[threadIdx.x] = ok;
+    }
+    __syncthreads();
+
+    const int nout = args.nsamples / args.tscrunch;
+    const int tp = blockIdx.x * blockDim.x + threadIdx.x;
+    const int f  = blockIdx.y;
+    if(tp >= nout) return;
+    const int t0 = tp * args.tscrunch;
+    const size_t P = 2;
+    long long S[kMaxBs], B[kMaxBs];
+#pragma unroll
+    for(int s = 0; s < kMaxBs; ++s) { S[s] = 0; B[s] = 0; }
+
+    const bool words = (args.tscrunch % 4) == 0;
+    for(int a = 0; a < args.nant; ++a) {
+        const uint8_t* r0 = args.fpact + (((size_t)f * P + 0) * args.nant + a) * 2 * args.row_stride + args.offset + t0;
+        const uint8_t* r1 = args.fpact + (((size_t)f * P + 1) * args.nant + a) * 2 * args.row_stride + args.offset + t0;
+        int pI = 0, pQ = 0, pU = 0, pV = 0;
+        if(words) {
+            for(int k = 0; k < args.tscrunch; k += 4) {
+                const int xr0 = *reinterpret_cast<const int*>(r0 + k);
+                const int xi0 = *reinterpret_cast<const int*>(r0 + args.row_stride + k);
+                const int xr1 = *reinterpret_cast<const int*>(r1 + k);
+                const int xi1 = *reinterpret_cast<const int*>(r1 + args.row_stride + k);
+                const int e0 = __dp4a(xi0, xi0, __dp4a(xr0, xr0, 0));
+                const int e1 = __dp4a(xi1, xi1, __dp4a(xr1, xr1, 0));
+                pI += e0 + e1;
+                pQ += e0 - e1;
+                pU += __dp4a(xi0, xi1, __dp4a(xr0, xr1, 0));
+                pV += __dp4a(xi0, xr1, 0) - __dp4a(xr0, xi1, 0);
+            }
+        } else {
+            for(int k = 0; k < args.tscrunch; ++k) {
+                const int xr0 = (int8_t)r0[k], xi0 = (int8_t)r0[args.row_stride + k];
+                const int xr1 = (int8_t)r1[k], xi1 = (int8_t)r1[args.row_stride + k];
+                const int e0 = xr0 * xr0 + xi0 * xi0, e1 = xr1 * xr1 + xi1 * xi1;
+                pI += e0 + e1;
+                pQ += e0 - e1;
+                pU += xr0 * xr1 + xi0 * xi1;
+                pV += xi0 * xr1 - xr0 * xi1;
+            }
+        }
+        const int pv = args.stokes == 0 ? pI : args.stokes == 1 ? pQ
+                     : args.stokes == 2 ? 2 * pU : 2 * pV;
+#pragma unroll
+        for(int s = 0; s < kMaxBs; ++s) {
+            const float w = sw[s][a];
+            const int wi = (int)w;
+            S[s] += (long long)wi * pv;
+            B[s] += (long long)abs(wi) * pI;  // |Q|,|U|,|V| <= I per sample
+        }
+    }
+
+    for(int s = 0; s < nbs; ++s) {
+        float power;
+        if(s_intw[s] && B[s] <= (1ll << 24)) {
+            power = (float)S[s];  // the float chain is exact
+        } else {
+            // reference order: t outer, a inner, float multiply and add
+            power = 0.0f;
+            for(int t = t0; t < t0 + args.tscrunch; ++t)
+                for(int a = 0; a < args.nant; ++a) {
+                    const uint8_t* q0 = args.fpact + (((size_t)f * P + 0) * args.nant + a) * 2 * args.row_stride + args.offset + t;
+                    const uint8_t* q1 = args.fpact + (((size_t)f * P + 1) * args.nant + a) * 2 * args.row_stride + args.offset + t;
+                    const float st = stokes_f(args.stokes, (float)(int8_t)q0[0],
+                                              (float)(int8_t)q0[args.row_stride],
+                                              (float)(int8_t)q1[0],
+                                              (float)(int8_t)q1[args.row_stride]);
+                    power = fadd(power, fmul(st, sw[s][a]));
+                }
+        }
+        const int bs = bs0 + s;
+        const size_t o  = ((size_t)bs * nout + tp) * args.nchans + f;
+        const size_t so = (size_t)bs * args.nchans + f;
+        args.raw[o] = power;
+        const float sc = args.stokes == 0
+                             ? rintf(fdiv(fsub(power, args.offset_v[so]), args.scale[so]))
+                             : rintf(fdiv(power, args.scale[so]));
+        args.out[o] = clamp_i8(sc);
+    }
+}
+
+}  // namespace
+
+int launch_incoherent_beamform(const void* d_fpact, size_t row_stride,
+                               size_t sample_offset, int nchans, int nsamples,
+                               int nant, int tscrunch, const float* d_scale,
+                               const float* d_offset,
+                               const float* d_beamset_weights, int nbeamsets,
+                               int stokes, float* d_raw, int8_t* d_out,
+                               cudaStream_t stream)
+{
+    SW_REQUIRE(d_fpact && d_scale && d_offset && d_beamset_weights && d_raw && d_out,
+               "sw_incoherent_beamform: null pointer");
+    SW_REQUIRE(nbeamsets > 0, "Number of beamsets must be greater than zero");
+    SW_REQUIRE(nant > 0 && nant <= kMaxAnt, "sw_incoherent_beamform: bad antenna count");
+    SW_REQUIRE(tscrunch > 0 && nsamples % tscrunch == 0,
+               "sw_incoherent_beamform: nsamples must be a multiple of tscrunch");
+    SW_REQUIRE(stokes >= 0 && stokes <= 3, "sw_incoherent_beamform: bad Stokes mode");
+    SW_REQUIRE(tscrunch % 4 != 0 || (row_stride % 4 == 0 && sample_offset % 4 == 0),
+               "sw_incoherent_beamform: stride/offset must be multiples of 4");
+    SW_REQUIRE(nchans > 0 && nchans <= 65535, "sw_incoherent_beamform: bad channel count");
+    IbArgs args{static_cast<const uint8_t*>(d_fpact), row_stride, sample_offset,
+                nchans, nsamples, nant, tscrunch, nbeamsets, stokes, d_scale,
+                d_offset, d_beamset_weights, d_raw, d_out};
+    const int nout = nsamples / tscrunch;
+    dim3 grid(cdiv(nout, 128), nchans);
+    for(int bs0 = 0; bs0 < nbeamsets; bs0 += kMaxBs) {
+        ib_k<<<grid, 128, 0, stream>>>(args, bs0);
+        SW_LAUNCH_CHECK();
+    }
+    return SW_OK;
+}
+
+}  // namespace swb
+
+extern "C" int sw_incoherent_beamform(const void* d_fpact, size_t row_stride,
+                                      size_t sample_offset, int nchans,
+                                      int nsamples, int nant, int tscrunch,
+                                      const float* d_scale, const float* d_offset,
+                                      const float* d_beamset_weights,
+                                      int nbeamsets, int stokes, float* d_raw,
+                                      int8_t* d_out, sw_stream_t stream)
+{
+    return swb::launch_incoherent_beamform(
+        d_fpact, row_stride, sample_offset, nchans, nsamples, nant, tscrunch,
+        d_scale, d_offset, d_beamset_weights, nbeamsets, stokes, d_raw, d_out,
+        swb::as_cuda(stream));
+}

@@ -1,0 +1,207 @@
+// StatisticsCalculator on the B200.
+//
+// The reference (cpp/skyweaver/src/StatisticsCalculator.cu:54-85) walks each
+// (channel, pol, antenna) series serially in one thread with FP64 running
+// moments.  Here the int8 inputs make the raw power sums S1..S4 exact in
+// 64-bit integers, so the series is split over many CTAs that add their
+// partial sums into an int64 workspace, and a finalize kernel forms mean,
+// std (n-1), skewness and kurtosis in FP64 from the exact sums.  The kernel
+// streams the FPACT rows once with 16-byte loads (HBM bound).
+//
+// update_scalings (cpp/skyweaver/src/StatisticsCalculator.cu:132-239) runs
+// on the device with the same IEEE single operations in the same order; its
+// outputs are indexed [beamset][chan] (the reference writes [chan] for every
+// beamset).
+#include "sw_common.cuh"
+
+namespace swb {
+namespace {
+
+constexpr int kStatsThreads = 256;
+constexpr int kChunkSamples = 16384;  // samples per CTA per row pair
+
+__device__ __forceinline__ void accum_word(uint32_t w, int& s1, int& s2,
+                                           long long& s3, long long& s4)
+{
+    s1 = __dp4a((int)w, 0x01010101, s1);
+    s2 = __dp4a((int)w, (int)w, s2);
+#pragma unroll
+    for(int k = 0; k < 4; ++k) {
+        const int x  = (int)(int8_t)(w >> (8 * k));
+        const int x2 = x * x;
+        s3 += (long long)(x2 * x);
+        s4 += (long long)x2 * x2;
+    }
+}
+
+// grid: (chunks per series, F*P*A series).  Each series is the pair of
+// planar rows (re, im) of one (f, p, a).
+__global__ void __launch_bounds__(kStatsThreads)
+stats_partial_k(const uint8_t* __restrict__ fpact, size_t row_stride,
+                size_t sample_offset, int nsamples,
+                unsigned long long* __restrict__ sums)
+{
+    const size_t series = blockIdx.y;
+    const int t0 = blockIdx.x * kChunkSamples;
+    const int t1 = min(nsamples, t0 + kChunkSamples);
+    int s1 = 0, s2 = 0;
+    long long s3 = 0, s4 = 0;
+    for(int c = 0; c < 2; ++c) {
+        const uint8_t* row = fpact + (series * 2 + c) * row_stride + sample_offset;
+        for(int t = t0 + threadIdx.x * 16; t < t1; t += kStatsThreads * 16) {
+            const uint4 v = *reinterpret_cast<const uint4*>(row + t);
+            accum_word(v.x, s1, s2, s3, s4);
+            accum_word(v.y, s1, s2, s3, s4);
+            accum_word(v.z, s1, s2, s3, s4);
+            accum_word(v.w, s1, s2, s3, s4);
+        }
+    }
+    long long v1 = s1, v2 = s2, v3 = s3, v4 = s4;
+#pragma unroll
+    for(int o = 16; o > 0; o >>= 1) {
+        v1 += __shfl_xor_sync(0xffffffffu, v1, o);
+        v2 += __shfl_xor_sync(0xffffffffu, v2, o);
+        v3 += __shfl_xor_sync(0xffffffffu, v3, o);
+        v4 += __shfl_xor_sync(0xffffffffu, v4, o);
+    }
+    __shared__ long long red[kStatsThreads / 32][4];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if(lane == 0) {
+        red[warp][0] = v1; red[warp][1] = v2; red[warp][2] = v3; red[warp][3] = v4;
+    }
+    __syncthreads();
+    if(threadIdx.x < 4) {
+        long long acc = 0;
+        for(int w = 0; w < kStatsThreads / 32; ++w) acc += red[w][threadIdx.x];
+        atomicAdd(&sums[series * 4 + threadIdx.x], (unsigned long long)acc);
+    }
+}
+
+__global__ void stats_finalize_k(const long long* __restrict__ sums,
+                                 float4* __restrict__ stats, int nseries,
+                                 int nsamples)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= nseries) return;
+    const double n  = 2.0 * nsamples;
+    const double S1 = (double)sums[4 * i + 0];
+    const double S2 = (double)sums[4 * i + 1];
+    const double S3 = (double)sums[4 * i + 2];
+    const double S4 = (double)sums[4 * i + 3];
+    const double m  = S1 / n;
+    const double M2 = S2 - S1 * m;
+    const double M3 = S3 - 3.0 * m * S2 + 3.0 * m * m * S1 - n * m * m * m;
+    const double M4 = S4 - 4.0 * m * S3 + 6.0 * m * m * S2 - 4.0 * m * m * m * S1 +
+                      n * m * m * m * m;
+    float4 r;
+    r.x = (float)m;
+    r.y = (float)sqrt(M2 / (n - 1.0));
+    r.z = (float)(sqrt(n) * M3 / pow(M2, 1.5));
+    r.w = (float)(n * M4 / (M2 * M2) - 3.0);
+    stats[i] = r;
+}
+
+// One thread per (beamset, channel); sequential over (pol, antenna) exactly
+// like the reference's host loop.
+__global__ void scalings_k(const float4* __restrict__ stats,
+                           const float* __restrict__ bw, int nbeamsets,
+                           int nchans, int npol, int nant, int cb_tscrunch,
+                           int ib_tscrunch, float output_level,
+                           float* __restrict__ cb_off, float* __restrict__ cb_scl,
+                           float* __restrict__ ib_off, float* __restrict__ ib_scl)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= nbeamsets * nchans) return;
+    const int s = i / nchans, f = i % nchans;
+    float sum = 0.0f, count = 0.0f;
+    for(int p = 0; p < npol; ++p)
+        for(int a = 0; a < nant; ++a) {
+            const float w = bw[(size_t)nant * s + a];
+            sum   = fadd(sum, fmul(w, stats[((size_t)f * npol + p) * nant + a].y));
+            count = fadd(count, w);
+        }
+    const float avg_std = fdiv(sum, count);
+    const float eff     = fdiv(count, (float)npol);
+    {
+        const float x     = fmul(fmul(127.0f, avg_std), sqrtf(eff));
+        const float scale = fmul(x, x);
+        const float dof   = (float)(2 * cb_tscrunch * npol);
+        cb_off[i] = fmul(scale, dof);
+        cb_scl[i] = fdiv(fmul(scale, sqrtf(fmul(2.0f, dof))), output_level);
+    }
+    {
+        const float scale = fmul(avg_std, avg_std);
+        const float dof   = fmul(fmul((float)(2 * ib_tscrunch), eff), (float)npol);
+        ib_off[i] = fmul(scale, dof);
+        ib_scl[i] = fdiv(fmul(scale, sqrtf(fmul(2.0f, dof))), output_level);
+    }
+}
+
+}  // namespace
+
+int launch_statistics(const void* d_fpact, size_t row_stride,
+                      size_t sample_offset, int nchans, int npol, int nant,
+                      int nsamples, void* d_scratch, float* d_stats,
+                      cudaStream_t stream)
+{
+    SW_REQUIRE(d_fpact && d_scratch && d_stats, "sw_statistics: null pointer");
+    SW_REQUIRE(nsamples > 0 && nsamples % 16 == 0,
+               "sw_statistics: nsamples must be a positive multiple of 16");
+    SW_REQUIRE(row_stride % 16 == 0 && sample_offset % 16 == 0,
+               "sw_statistics: stride and offset must be multiples of 16");
+    const int nseries = nchans * npol * nant;
+    SW_REQUIRE(nseries > 0 && nseries <= 65535, "sw_statistics: too many series");
+    const size_t sum_bytes = (size_t)nseries * 4 * sizeof(long long);
+    SW_CUDA_CHECK(cudaMemsetAsync(d_scratch, 0, sum_bytes, stream));
+    dim3 grid(cdiv(nsamples, kChunkSamples), nseries);
+    stats_partial_k<<<grid, kStatsThreads, 0, stream>>>(
+        static_cast<const uint8_t*>(d_fpact), row_stride, sample_offset,
+        nsamples, static_cast<unsigned long long*>(d_scratch));
+    SW_LAUNCH_CHECK();
+    stats_finalize_k<<<cdiv(nseries, 256), 256, 0, stream>>>(
+        static_cast<const long long*>(d_scratch),
+        reinterpret_cast<float4*>(d_stats), nseries, nsamples);
+    SW_LAUNCH_CHECK();
+    return SW_OK;
+}
+
+}  // namespace swb
+
+using namespace swb;
+
+extern "C" {
+
+size_t sw_statistics_scratch_bytes(int nchans, int npol, int nant)
+{
+    return (size_t)nchans * npol * nant * 4 * sizeof(long long);
+}
+
+int sw_statistics(const void* d_fpact, size_t row_stride, size_t sample_offset,
+                  int nchans, int npol, int nant, int nsamples,
+                  void* d_scratch, float* d_stats, sw_stream_t stream)
+{
+    return launch_statistics(d_fpact, row_stride, sample_offset, nchans, npol,
+                             nant, nsamples, d_scratch, d_stats, as_cuda(stream));
+}
+
+int sw_update_scalings(const float* d_stats, const float* d_beamset_weights,
+                       int nbeamsets, int nchans, int npol, int nant,
+                       int cb_tscrunch, int ib_tscrunch, float output_level,
+                       float* d_cb_offsets, float* d_cb_scaling,
+                       float* d_ib_offsets, float* d_ib_scaling,
+                       sw_stream_t stream)
+{
+    SW_REQUIRE(d_stats && d_beamset_weights && d_cb_offsets && d_cb_scaling &&
+                   d_ib_offsets && d_ib_scaling,
+               "sw_update_scalings: null pointer");
+    SW_REQUIRE(nbeamsets > 0 && nchans > 0, "sw_update_scalings: empty shape");
+    const int n = nbeamsets * nchans;
+    scalings_k<<<cdiv(n, 128), 128, 0, as_cuda(stream)>>>(
+        reinterpret_cast<const float4*>(d_stats), d_beamset_weights, nbeamsets,
+        nchans, npol, nant, cb_tscrunch, ib_tscrunch, output_level,
+        d_cb_offsets, d_cb_scaling, d_ib_offsets, d_ib_scaling);
+    SW_LAUNCH_CHECK();
+    return SW_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,304 @@
+"""Python face of the skyweaver_b200 C ABI, shaped like the reference's stage
+classes (Transposer, StatisticsCalculator, WeightsManager, CoherentDedisperser,
+IncoherentBeamformer, CoherentBeamformer, IncoherentDedisperser,
+BeamformerPipeline).  Device memory is torch CUDA tensors; every call goes
+through libskyweaver_b200.so (there is no other implementation).
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import STOKES, CbProblem, CbShape, call, lib
+
+DM_CONST = 4.148806423e15
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def _stream(stream=None):
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def channel_frequencies(centre, bandwidth, nchans):
+    chbw = bandwidth / nchans
+    return centre - bandwidth / 2.0 + chbw / 2.0 + chbw * np.arange(nchans)
+
+
+# ------------------------------------------------------------------ layouts
+def transpose_ftpa(taftp: torch.Tensor, out_nant: int, stream=None) -> torch.Tensor:
+    """Transposer::transpose: TAFTP [H][A_in][F][256][2][2] -> FTPA."""
+    H, A_in, F = taftp.shape[:3]
+    out = torch.empty((F, H * 256, 2, out_nant, 2), dtype=torch.int8, device=taftp.device)
+    call("sw_transpose_ftpa", _ptr(taftp), _ptr(out), H, A_in, out_nant, F, _stream(stream))
+    return out
+
+
+def transpose_fpact(taftp, out_nant, row_stride=None, offset=0, out=None, stream=None):
+    H, A_in, F = taftp.shape[:3]
+    T = H * 256
+    row_stride = row_stride or (offset + T)
+    if out is None:
+        out = torch.zeros((F, 2, out_nant, 2, row_stride), dtype=torch.int8, device=taftp.device)
+    call("sw_transpose_fpact", _ptr(taftp), _ptr(out), H, A_in, out_nant, F, row_stride,
+         offset, _stream(stream))
+    return out
+
+
+def ftpa_to_fpact(ftpa, row_stride=None, offset=0, stream=None):
+    F, T, P, A, _ = ftpa.shape
+    row_stride = row_stride or (offset + T)
+    out = torch.zeros((F, P, A, 2, row_stride), dtype=torch.int8, device=ftpa.device)
+    call("sw_ftpa_to_fpact", _ptr(ftpa), _ptr(out), F, T, A, row_stride, offset,
+         _stream(stream))
+    return out
+
+
+def fpact_to_ftpa(fpact, nsamples, offset=0, stream=None):
+    F, P, A, _, stride = fpact.shape
+    out = torch.empty((F, nsamples, P, A, 2), dtype=torch.int8, device=fpact.device)
+    call("sw_fpact_to_ftpa", _ptr(fpact), _ptr(out), F, nsamples, A, stride, offset,
+         _stream(stream))
+    return out
+
+
+# --------------------------------------------------------------- statistics
+def statistics(fpact, nsamples, offset=0, stream=None):
+    """StatisticsCalculator::calculate_statistics -> float [F][P][A][4]."""
+    F, P, A, _, stride = fpact.shape
+    scratch = torch.empty(lib().sw_statistics_scratch_bytes(F, P, A), dtype=torch.uint8,
+                          device=fpact.device)
+    stats = torch.empty((F, P, A, 4), dtype=torch.float32, device=fpact.device)
+    call("sw_statistics", _ptr(fpact), stride, offset, F, P, A, nsamples, _ptr(scratch),
+         _ptr(stats), _stream(stream))
+    return stats
+
+
+def update_scalings(stats, beamset_weights, cb_tscrunch, ib_tscrunch, output_level,
+                    stream=None):
+    """StatisticsCalculator::update_scalings -> (cb_off, cb_scl, ib_off, ib_scl)."""
+    F, P, A, _ = stats.shape
+    S = beamset_weights.shape[0]
+    outs = [torch.empty(S * F, dtype=torch.float32, device=stats.device) for _ in range(4)]
+    call("sw_update_scalings", _ptr(stats), _ptr(beamset_weights), S, F, P, A, cb_tscrunch,
+         ib_tscrunch, ctypes.c_float(output_level), *[_ptr(o) for o in outs], _stream(stream))
+    return tuple(outs)
+
+
+# ------------------------------------------------------------------ weights
+def generate_weights(delays, freqs, current_epoch, delay_epoch, want_fba=True,
+                     want_gemm=True, stream=None):
+    """WeightsManager::weights: float3 [B][A] -> (char2 [F][B][A], GEMM layout)."""
+    B, A, _ = delays.shape
+    F = freqs.shape[0]
+    fba = torch.empty((F, B, A, 2), dtype=torch.int8, device=delays.device) if want_fba else None
+    gemm = (torch.empty((F, 2, B, A, 2), dtype=torch.int8, device=delays.device)
+            if want_gemm else None)
+    call("sw_generate_weights", _ptr(delays), _ptr(freqs), A, B, F,
+         ctypes.c_double(current_epoch), ctypes.c_double(delay_epoch), _ptr(fba), _ptr(gemm),
+         _stream(stream))
+    return fba, gemm
+
+
+def pack_weights(fba, stream=None):
+    F, B, A, _ = fba.shape
+    gemm = torch.empty((F, 2, B, A, 2), dtype=torch.int8, device=fba.device)
+    call("sw_pack_weights", _ptr(fba), _ptr(gemm), F, B, A, _stream(stream))
+    return gemm
+
+
+# --------------------------------------------------------------------- beams
+def incoherent_beamform(fpact, nsamples, tscrunch, scale, offset, beamset_weights,
+                        offset_samples=0, stokes="I", stream=None):
+    F, P, A, _, stride = fpact.shape
+    S = beamset_weights.shape[0]
+    raw = torch.empty((S, nsamples // tscrunch, F), dtype=torch.float32, device=fpact.device)
+    out = torch.empty((S, nsamples // tscrunch, F), dtype=torch.int8, device=fpact.device)
+    call("sw_incoherent_beamform", _ptr(fpact), stride, offset_samples, F, nsamples, A,
+         tscrunch, _ptr(scale), _ptr(offset), _ptr(beamset_weights), S, STOKES[stokes],
+         _ptr(raw), _ptr(out), _stream(stream))
+    return raw, out
+
+
+def cb_shape(fpact, nsamples, nbeams, tscrunch, stokes="I", ib_subtract=True,
+             offset_samples=0):
+    F, P, A, _, stride = fpact.shape
+    return CbShape(F, nsamples, A, nbeams, tscrunch, STOKES[stokes], int(ib_subtract),
+                   stride, offset_samples)
+
+
+def coherent_beamform(fpact, weights_gemm, scale, offset, mapping, ib_raw, nsamples,
+                      tscrunch, stokes="I", ib_subtract=True, beam_start=0, beam_count=None,
+                      out=None, debug=False, offset_samples=0, stream=None):
+    """CoherentBeamformer::beamform (plain: one problem) -> int8 TFB."""
+    F = fpact.shape[0]
+    nbeams = weights_gemm.shape[2]
+    beam_count = nbeams if beam_count is None else beam_count
+    if out is None:
+        out = torch.zeros((nsamples // tscrunch, F, nbeams), dtype=torch.int8,
+                          device=fpact.device)
+    dbg = (torch.zeros((F, nsamples, 2, nbeams, 2), dtype=torch.int32, device=fpact.device)
+           if debug else None)
+    shape = cb_shape(fpact, nsamples, nbeams, tscrunch, stokes, ib_subtract, offset_samples)
+    prob = CbProblem(fpact.data_ptr(), out.data_ptr(),
+                     ib_raw.data_ptr() if ib_raw is not None else None, beam_start, beam_count)
+    call("sw_coherent_beamform", ctypes.byref(shape), ctypes.byref(prob), _ptr(weights_gemm),
+         _ptr(scale), _ptr(offset), _ptr(mapping), _ptr(dbg), _stream(stream))
+    return (out, dbg) if debug else out
+
+
+def coherent_beamform_grouped(problems, weights_gemm, scale, offset, mapping, nsamples,
+                              tscrunch, stokes="I", ib_subtract=True, offset_samples=0,
+                              stream=None):
+    """problems: list of (fpact, out, ib_raw, beam_start, beam_count)."""
+    fp0 = problems[0][0]
+    nbeams = weights_gemm.shape[2]
+    shape = cb_shape(fp0, nsamples, nbeams, tscrunch, stokes, ib_subtract, offset_samples)
+    arr = (CbProblem * len(problems))(*[
+        CbProblem(p[0].data_ptr(), p[1].data_ptr(), p[2].data_ptr() if p[2] is not None else None,
+                  p[3], p[4]) for p in problems])
+    call("sw_coherent_beamform_grouped", ctypes.byref(shape), arr, len(problems),
+         _ptr(weights_gemm), _ptr(scale), _ptr(offset), _ptr(mapping), _stream(stream))
+
+
+# ------------------------------------------------------- coherent dedisp.
+def dm_delay(f_ref, f, dm):
+    return DM_CONST * (1 / (f_ref * f_ref) - 1 / (f * f)) * dm
+
+
+class CoherentDedisperser:
+    """create_coherent_dedisperser_config + CoherentDedisperser::dedisperse for
+    all channels/antennas/pols and DMs of a gulp (overlap-save with history)."""
+
+    def __init__(self, nchans, nant, fft_len, overlap, low_freq, bw, dms, device="cuda"):
+        self.nchans, self.nant, self.fft_len, self.overlap = nchans, nant, fft_len, overlap
+        self.dms = np.asarray(dms, np.float32)
+        nbytes = lib().sw_cdd_setup_bytes(len(dms), nchans, fft_len)
+        if nbytes == 0:
+            raise ValueError(f"unsupported fft_len {fft_len}")
+        self.setup = torch.empty(nbytes, dtype=torch.uint8, device=device)
+        dms_c = (ctypes.c_float * len(dms))(*self.dms)
+        call("sw_cdd_chirps", dms_c, len(dms), nchans, fft_len, ctypes.c_double(low_freq),
+             ctypes.c_double(bw), _ptr(self.setup), _stream())
+
+    def dedisperse(self, fpact_ext, nsamples, outs=None, stream=None):
+        """fpact_ext rows hold `overlap` history samples then the gulp."""
+        F, P, A, _, stride = fpact_ext.shape
+        nd = len(self.dms)
+        if outs is None:
+            outs = [torch.empty((F, P, A, 2, nsamples), dtype=torch.int8,
+                                device=fpact_ext.device) for _ in range(nd)]
+        arr = (ctypes.c_void_p * nd)(*[o.data_ptr() for o in outs])
+        call("sw_coherent_dedisperse", _ptr(fpact_ext), stride, F, P, A, nsamples,
+             self.fft_len, self.overlap, _ptr(self.setup), nd, arr, outs[0].shape[-1],
+             _stream(stream))
+        return outs
+
+
+# ----------------------------------------------------- incoherent dedisp.
+def incoherent_dedisperse(tfb, delays, max_delay, tscrunch, scale_factor, stream=None):
+    T, F, B = tfb.shape
+    ndms = delays.shape[0]
+    out = torch.empty(((T - max_delay) // tscrunch, ndms, B), dtype=torch.int8,
+                      device=tfb.device)
+    call("sw_incoherent_dedisperse", _ptr(tfb), T, F, B, _ptr(delays), ndms, max_delay,
+         tscrunch, ctypes.c_float(scale_factor), _ptr(out), _stream(stream))
+    return out
+
+
+# ------------------------------------------------------------------ pipeline
+class BeamformerPipeline:
+    """sw_pipeline_*: the graph-captured per-gulp chain (BeamformerPipeline)."""
+
+    def __init__(self, *, nantennas, input_nantennas, nchans, nbeams, gulp_samples,
+                 tscrunch, centre_frequency, bandwidth, dms, beamset_weights,
+                 beamset_mapping, stokes="I", ib_subtract=True, output_level=24.0,
+                 fft_len=0, coherent_dedispersion=True, grouped=True, use_graph=True):
+        self._dms = (ctypes.c_float * len(dms))(*[float(d) for d in dms])
+        bw = np.ascontiguousarray(beamset_weights, np.float32)
+        mp = np.ascontiguousarray(beamset_mapping, np.int32)
+        self._bw = bw.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+        self._mp = mp.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+        self._keep = (bw, mp)
+        cfg = _lib.PipelineConfig(
+            nantennas, input_nantennas, nchans, nbeams, gulp_samples, tscrunch,
+            STOKES[stokes], int(ib_subtract), output_level, centre_frequency, bandwidth,
+            len(dms), self._dms, fft_len, int(coherent_dedispersion), int(grouped),
+            int(use_graph), bw.shape[0], self._bw, self._mp)
+        h = ctypes.c_void_p()
+        call("sw_pipeline_create", ctypes.byref(cfg), ctypes.byref(h))
+        self.h = h
+        self.ndms = len(dms)
+        self.nchans, self.nbeams, self.tscrunch, self.gulp = nchans, nbeams, tscrunch, gulp_samples
+        self.nbeamsets = bw.shape[0]
+        self._nant = nantennas
+
+    def close(self):
+        if self.h:
+            lib().sw_pipeline_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_delays(self, delays: np.ndarray, delay_epoch: float):
+        d = np.ascontiguousarray(delays, np.float32)
+        call("sw_pipeline_set_delays", self.h, d.ctypes.data_as(ctypes.c_void_p),
+             ctypes.c_double(delay_epoch))
+
+    def process_device(self, taftp: torch.Tensor, epoch: float, stream=None):
+        call("sw_pipeline_process_device", self.h, _ptr(taftp), ctypes.c_double(epoch),
+             _stream(stream))
+
+    def process_host(self, taftp_pinned: torch.Tensor, epoch: float, cb_out_pinned=None,
+                     stream=None):
+        call("sw_pipeline_process_host", self.h, _ptr(taftp_pinned), ctypes.c_double(epoch),
+             _ptr(cb_out_pinned), _stream(stream))
+
+    def fft_plan(self):
+        n, o = ctypes.c_int(), ctypes.c_int()
+        call("sw_pipeline_fft_len", self.h, ctypes.byref(n), ctypes.byref(o))
+        return n.value, o.value
+
+    def cb_bytes_per_dm(self):
+        return lib().sw_pipeline_cb_bytes_per_dm(self.h)
+
+    def outputs(self, dm_idx: int):
+        """Copies of the last gulp's outputs for one DM (numpy)."""
+        pcb, praw, pib, pst = (ctypes.c_void_p() for _ in range(4))
+        call("sw_pipeline_outputs", self.h, dm_idx, ctypes.byref(pcb), ctypes.byref(praw),
+             ctypes.byref(pib), ctypes.byref(pst))
+        torch.cuda.synchronize()
+        T = self.gulp // self.tscrunch
+        S, F, B = self.nbeamsets, self.nchans, self.nbeams
+        res = {}
+        for name, p, dt, shape in (("cb", pcb, np.int8, (T, F, B)),
+                                   ("ib_raw", praw, np.float32, (S, T, F)),
+                                   ("ib", pib, np.int8, (S, T, F)),
+                                   ("stats", pst, np.float32, (F, 2, -1, 4))):
+            n = int(np.prod([x for x in shape if x > 0]))
+            if name == "stats":
+                n = F * 2 * (self._nant if hasattr(self, "_nant") else 0) * 4
+                if n == 0:
+                    continue
+            nbytes = n * np.dtype(dt).itemsize
+            res[name] = _device_view(p.value, nbytes).cpu().numpy().view(dt).reshape(shape)
+        return res
+
+
+def _device_view(ptr, nbytes):
+    # Build a uint8 CUDA tensor aliasing `ptr` (owned by the pipeline).
+    class _Arr:
+        __cuda_array_interface__ = {"shape": (nbytes,), "typestr": "|u1",
+                                    "data": (ptr, False), "version": 3}
+    return torch.as_tensor(_Arr(), device="cuda")

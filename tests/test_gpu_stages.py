@@ -1,0 +1,323 @@
+"""GPU parity tests: every CUDA stage against the oracle (a C restatement of
+the reference's CPU test implementations) on the same seeded inputs.
+
+Tolerances follow the reference's own tests and are written next to each
+check: integer/byte stages are bit-exact; the tensor-core beamformer's int32
+voltages are bit-exact and its int8 output is identical; statistics within
+1e-5 relative (StatisticsCalculatorTester.cu:157-169); coherent
+dedispersion within +-1 int8 LSB of the FP64 oracle
+(CoherentDedisperserTester.cu:195-203).
+"""
+import math
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev(cuda, a):
+    return cuda.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def _np(t):
+    return t.cpu().numpy()
+
+
+# ------------------------------------------------------------ transposer
+@pytest.mark.parametrize("in_nant,nheaps,out_nant", [(12, 12, 16), (16, 16, 64), (64, 3, 64)])
+def test_transpose_ftpa_exact(cuda, oracle, in_nant, nheaps, out_nant):
+    from skyweaver_b200 import stages, synthetic
+    g = synthetic.rng(1 + in_nant)
+    taftp = synthetic.voltages_taftp(g, nheaps, in_nant, 8, sigma=40)
+    ref = oracle.transpose(taftp, out_nant)
+    got = _np(stages.transpose_ftpa(_dev(cuda, taftp), out_nant))
+    assert np.array_equal(got, ref)  # TransposerTester.cu:89-92 exact
+
+
+def test_transpose_fpact_matches_ftpa(cuda, oracle):
+    from skyweaver_b200 import stages, synthetic
+    g = synthetic.rng(7)
+    taftp = synthetic.voltages_taftp(g, 4, 57, 4, sigma=30)
+    ref = oracle.transpose(taftp, 64)                     # FTPA [F][T][P][A][2]
+    fp = stages.transpose_fpact(_dev(cuda, taftp), 64, row_stride=1024 + 32, offset=32)
+    got = _np(fp)[..., 32:32 + 1024]                      # [F][P][A][C][T]
+    assert np.array_equal(got, ref.transpose(0, 2, 3, 4, 1))
+    back = _np(stages.fpact_to_ftpa(fp, 1024, offset=32))
+    assert np.array_equal(back, ref)
+
+
+def test_keep_history(cuda):
+    from skyweaver_b200._lib import call
+    import ctypes
+    rows, hist, T = 6, 32, 96
+    a = np.arange(rows * (hist + T), dtype=np.int64).astype(np.int8).reshape(rows, hist + T)
+    d = _dev(cuda, a)
+    call("sw_fpact_keep_history", ctypes.c_void_p(d.data_ptr()), rows, hist + T, hist,
+         ctypes.c_void_p(cuda.cuda.current_stream().cuda_stream))
+    got = _np(d)
+    assert np.array_equal(got[:, :hist], a[:, T:T + hist])
+    assert np.array_equal(got[:, hist:], a[:, hist:])
+
+
+# ------------------------------------------------------------ statistics
+def test_statistics(cuda, oracle):
+    from skyweaver_b200 import stages, synthetic
+    g = synthetic.rng(1337)
+    taftp = synthetic.voltages_taftp(g, 8, 64, 4, sigma=20)   # StatisticsCalculatorTester: sigma 20
+    ftpa = oracle.transpose(taftp, 64)
+    ref = oracle.statistics(ftpa)
+    fp = stages.transpose_fpact(_dev(cuda, taftp), 64, row_stride=2048 + 64, offset=64)
+    got = _np(stages.statistics(fp, 2048, offset=64))
+    np.testing.assert_allclose(got, ref, rtol=1e-5, atol=1e-6)
+
+
+def test_scalings_bit_exact(cuda, oracle):
+    from skyweaver_b200 import stages, synthetic
+    g = synthetic.rng(5)
+    stats = np.abs(g.normal(8, 2, size=(16, 2, 32, 4))).astype(np.float32)
+    bw = synthetic.beamset_masks(g, 32, [32, 20, 7])
+    ref = oracle.scalings(stats, bw, 3, 16, 8, 24.0)
+    got = stages.update_scalings(_dev(cuda, stats), _dev(cuda, bw), 16, 8, 24.0)
+    for r, x in zip(ref, got):
+        assert np.array_equal(_np(x), r)
+
+
+# --------------------------------------------------------------- weights
+@pytest.mark.parametrize("case", ["zero", "real_value", "real_values", "synthetic"])
+def test_weights(cuda, oracle, case):
+    from skyweaver_b200 import stages, synthetic
+    B, A, F = 64, 64, 16
+    freqs = synthetic.channel_frequencies(1284e6, 13.375e6, F)
+    if case == "zero":          # WeightsManagerTester.cu:99-112
+        d = np.tile(np.array([1.0, 0.0, 0.0], np.float32), (B, A, 1))
+    elif case == "real_value":  # :114-127
+        d = np.tile(np.array([1.0, 1e-11, 1e-10], np.float32), (B, A, 1))
+    elif case == "real_values":  # :129-145
+        ii = np.arange(B * A, dtype=np.float32)
+        d = np.stack([ii * np.float32(1e-11), ii * np.float32(1e-15),
+                      np.zeros_like(ii)], -1).reshape(B, A, 3).astype(np.float32)
+    else:
+        d = synthetic.delay_model(synthetic.rng(3), B, A)
+    ref = oracle.weights(d, freqs, 10.0, 9.0)
+    fba, gemm = stages.generate_weights(_dev(cuda, d), _dev(cuda, freqs), 10.0, 9.0)
+    got = _np(fba)
+    # exact except where the reference's round-half-away and the GPU's
+    # round-half-even differ on an exact .5 (not present in these inputs)
+    assert np.array_equal(got, ref)
+    gm = _np(gemm)
+    assert np.array_equal(gm[:, 0, ..., 0], ref[..., 0])
+    assert np.array_equal(gm[:, 0, ..., 1], -ref[..., 1])
+    assert np.array_equal(gm[:, 1, ..., 0], ref[..., 1])
+    assert np.array_equal(gm[:, 1, ..., 1], ref[..., 0])
+    assert np.array_equal(_np(stages.pack_weights(fba)), gm)
+
+
+# ----------------------------------------------------- incoherent beam
+@pytest.mark.parametrize("stokes", ["I", "Q", "U", "V"])
+@pytest.mark.parametrize("nbeamsets", [1, 4])
+def test_incoherent_beam_bit_exact(cuda, oracle, stokes, nbeamsets):
+    from skyweaver_b200 import stages, synthetic
+    g = synthetic.rng(11)
+    A, F, H, ts = 64, 4, 4, 16
+    taftp = synthetic.voltages_taftp(g, H, A, F, sigma=32)   # IncoherentBeamformerTester: sigma 32
+    ftpa = oracle.transpose(taftp, A)
+    T = H * 256
+    level = 32.0
+    dof = 2 * ts * A * 2
+    scale = np.full(nbeamsets * F, level ** 2 * math.sqrt(2 * dof) / level, np.float32)
+    offset = np.full(nbeamsets * F, level ** 2 * dof, np.float32)
+    bw = synthetic.beamset_masks(g, A, [64, 40, 17, 3][:nbeamsets])
+    raw_ref, out_ref = oracle.incoherent_beam(ftpa, ts, scale, offset, bw, nbeamsets, stokes)
+    fp = stages.transpose_fpact(_dev(cuda, taftp), A)
+    raw, out = stages.incoherent_beamform(fp, T, ts, _dev(cuda, scale), _dev(cuda, offset),
+                                          _dev(cuda, bw), stokes=stokes)
+    assert np.array_equal(_np(raw), raw_ref)
+    assert np.array_equal(_np(out), out_ref)
+
+
+def test_incoherent_beam_float_chain_path(cuda, oracle):
+    """Strong RFI and non-integer weights force the reference-order float chain."""
+    from skyweaver_b200 import stages, synthetic
+    g = synthetic.rng(12)
+    A, F, H, ts = 64, 2, 2, 32
+    taftp = synthetic.voltages_taftp(g, H, A, F, sigma=8)
+    synthetic.inject_tones(taftp, [1], amplitude=110.0)
+    ftpa = oracle.transpose(taftp, A)
+    bw = np.stack([np.ones(A, np.float32), g.uniform(0.3, 1.0, A).astype(np.float32)])
+    scale = np.full(2 * F, 5000.0, np.float32)
+    offset = np.full(2 * F, 1e5, np.float32)
+    raw_ref, out_ref = oracle.incoherent_beam(ftpa, ts, scale, offset, bw, 2)
+    fp = stages.transpose_fpact(_dev(cuda, taftp), A)
+    raw, out = stages.incoherent_beamform(fp, H * 256, ts, _dev(cuda, scale),
+                                          _dev(cuda, offset), _dev(cuda, bw))
+    assert np.array_equal(_np(raw), raw_ref)
+    assert np.array_equal(_np(out), out_ref)
+
+
+# ------------------------------------------------------- coherent beam
+def _cb_case(cuda, oracle, A, B, F, H, ts, stokes, ib_sub, nbeamsets=2, seed=21):
+    from skyweaver_b200 import stages, synthetic
+    g = synthetic.rng(seed)
+    taftp = synthetic.voltages_taftp(g, H, A, F, sigma=32)
+    T = H * 256
+    ftpa = oracle.transpose(taftp, A)
+    # weights 127*exp(i theta) like CoherentBeamformerTester.cu:301-309
+    th = g.uniform(0, 2 * np.pi, size=(F, B, A))
+    w = np.stack([np.rint(127 * np.cos(th)), np.rint(127 * np.sin(th))], -1).astype(np.int8)
+    level = 32.0
+    cb_scale = (127 * level * math.sqrt(A)) ** 2
+    dof = 2 * ts * 2
+    scales = np.full(nbeamsets * F, cb_scale * math.sqrt(2 * dof) / level, np.float32)
+    offsets = np.full(nbeamsets * F, cb_scale * dof, np.float32)
+    bw = np.ones((nbeamsets, A), np.float32)
+    mapping = np.zeros(B, np.int32)
+    mapping[0] = 1 % nbeamsets                 # CoherentBeamformerTester.cu:259
+    ib_dof = 2 * ts * A * 2
+    ib_scale = np.full(nbeamsets * F, level ** 2 * math.sqrt(2 * ib_dof) / level, np.float32)
+    ib_off = np.full(nbeamsets * F, level ** 2 * ib_dof, np.float32)
+    fp = stages.transpose_fpact(_dev(cuda, taftp), A)
+    raw_ib, _ = stages.incoherent_beamform(fp, T, ts, _dev(cuda, ib_scale), _dev(cuda, ib_off),
+                                           _dev(cuda, bw), stokes=stokes)
+    gemm = stages.pack_weights(_dev(cuda, w))
+    out, dbg = stages.coherent_beamform(fp, gemm, _dev(cuda, scales), _dev(cuda, offsets),
+                                        _dev(cuda, mapping), raw_ib, T, ts, stokes=stokes,
+                                        ib_subtract=ib_sub, debug=True)
+    ref, volts = oracle.coherent_beam(ftpa, w, ts, scales, offsets, bw, mapping, stokes,
+                                      ib_sub, want_voltages=True)
+    return _np(out), ref, _np(dbg), volts
+
+
+@pytest.mark.parametrize("A", [16, 32, 64])
+def test_coherent_beam_voltages_and_power_exact(cuda, oracle, A):
+    out, ref, dbg, volts = _cb_case(cuda, oracle, A, 128, 2, 2, 16, "I", True)
+    assert np.array_equal(dbg, volts)     # int32 beam voltages bit-exact
+    assert np.array_equal(out, ref)       # int8 TFB identical to the CPU reference
+
+
+@pytest.mark.parametrize("stokes", ["I", "Q", "U", "V"])
+@pytest.mark.parametrize("ib_sub", [True, False])
+def test_coherent_beam_stokes(cuda, oracle, stokes, ib_sub):
+    out, ref, _, _ = _cb_case(cuda, oracle, 64, 256, 3, 2, 4, stokes, ib_sub, seed=22)
+    assert np.array_equal(out, ref)
+
+
+def test_coherent_beam_partial_block_and_tscrunch(cuda, oracle):
+    out, ref, _, _ = _cb_case(cuda, oracle, 64, 96, 2, 1, 32, "I", True, seed=23)
+    assert np.array_equal(out, ref)
+
+
+def test_coherent_beam_grouped_equals_plain(cuda, oracle):
+    from skyweaver_b200 import stages, synthetic
+    g = synthetic.rng(31)
+    A, B, F, H, ts = 64, 384, 2, 2, 16
+    T = H * 256
+    fps = [stages.transpose_fpact(_dev(cuda, synthetic.voltages_taftp(g, H, A, F)), A)
+           for _ in range(3)]
+    th = g.uniform(0, 2 * np.pi, size=(F, B, A))
+    w = np.stack([np.rint(127 * np.cos(th)), np.rint(127 * np.sin(th))], -1).astype(np.int8)
+    gemm = stages.pack_weights(_dev(cuda, w))
+    mapping = np.repeat(np.arange(3, dtype=np.int32), [200, 120, 64])
+    scales = _dev(cuda, np.full(3 * F, 1e6, np.float32))
+    offs = _dev(cuda, np.full(3 * F, 1e5, np.float32))
+    ibs = [cuda.rand((3, T // ts, F), device="cuda") * 100 for _ in fps]
+    plain = []
+    for fp, ib in zip(fps, ibs):
+        outs = cuda.zeros((T // ts, F, B), dtype=cuda.int8, device="cuda")
+        for b0, n in ((0, 200), (200, 120), (320, 64)):
+            stages.coherent_beamform(fp, gemm, scales, offs, _dev(cuda, mapping), ib, T, ts,
+                                     beam_start=b0, beam_count=n, out=outs)
+        plain.append(_np(outs))
+    outs = [cuda.zeros((T // ts, F, B), dtype=cuda.int8, device="cuda") for _ in fps]
+    probs = [(fp, o, ib, b0, n) for fp, o, ib in zip(fps, outs, ibs)
+             for b0, n in ((0, 200), (200, 120), (320, 64))]
+    stages.coherent_beamform_grouped(probs, gemm, scales, offs, _dev(cuda, mapping), T, ts)
+    for a, b in zip(plain, outs):
+        assert np.array_equal(a, _np(b))
+
+
+# ------------------------------------------------- coherent dedispersion
+def test_coherent_dedispersion_golden_vector(cuda):
+    """CoherentDedisperserTester.cu:113-204: DM 1000, fft 1024, 1 channel,
+    python-generated golden output, +-1 LSB."""
+    from skyweaver_b200 import stages
+    inp = np.fromfile(os.path.join(GOLDEN, "codedisp_input_DM1000_1chan.bin"),
+                      np.int8).reshape(1024, 2, 64, 2)
+    want = np.fromfile(os.path.join(GOLDEN, "codedisp_output_DM1000_1chan.bin"),
+                       np.int8).reshape(446, 2, 64, 2)
+    tsamp = 4096 / 856e6
+    overlap = math.ceil(stages.dm_delay(856e6, 856e6 + 856e6 / 4096, 1000.0) / tsamp)
+    assert overlap == 578
+    cdd = stages.CoherentDedisperser(64, 64, 1024, overlap, 856e6, 13.375e6, [0.0, 1000.0])
+    fp = _dev(cuda, inp.transpose(1, 2, 3, 0)[None].copy())   # [1][P][A][C][1024]
+    outs = cdd.dedisperse(fp, 1024 - overlap)
+    got = _np(outs[1])[0].transpose(3, 0, 1, 2)                # [446][P][A][C]
+    diff = np.abs(got.astype(int) - want.astype(int))
+    assert diff.max() <= 1                                     # reference tolerance
+    assert (diff > 0).mean() < 1e-3
+    # DM 0 is the identity shifted by overlap/2 (CoherentDedisperserTester.cu:69-111)
+    got0 = _np(outs[0])[0].transpose(3, 0, 1, 2)
+    assert np.abs(got0.astype(int) - inp[overlap // 2: overlap // 2 + 446].astype(int)).max() <= 1
+
+
+@pytest.mark.parametrize("fft_len,dms", [(2048, [0.0, 50.0, 150.0]), (4096, [0.0, 500.0]),
+                                         (8192, [150.0]), (1024, [30.0])])
+def test_coherent_dedispersion_overlap_save(cuda, oracle, fft_len, dms):
+    from skyweaver_b200 import stages, synthetic
+    g = synthetic.rng(fft_len)
+    F, A, T = 2, 4, 8192
+    chbw = 856e6 / 1024                      # MeerKAT L-band 1024-channel mode
+    bw = F * chbw
+    low = 1284e6 - 32 * chbw                 # bottom of a 64-channel subband
+    tsamp = 1.0 / chbw
+    smear = stages.dm_delay(low, low + bw / F, max(dms)) / tsamp
+    overlap = int(math.ceil(smear)) + 1 & ~1
+    assert overlap < fft_len
+    ext = np.clip(np.rint(g.normal(0, 12, size=(F, 2, A, 2, overlap + T))), -127, 127).astype(np.int8)
+    cdd = stages.CoherentDedisperser(F, A, fft_len, overlap, low, bw, dms)
+    outs = cdd.dedisperse(_dev(cuda, ext), T)
+    for d, dm in enumerate(dms):
+        chirps = oracle.chirp(F, fft_len, low, bw, dm)
+        ftpa_ext = ext.transpose(0, 4, 1, 2, 3)                  # [F][O+T][P][A][2]
+        ref, f64 = oracle.cdd_ftpa(ftpa_ext, T, chirps, overlap, want_f64=True)
+        got = _np(outs[d]).transpose(0, 4, 1, 2, 3)
+        diff = np.abs(got.astype(int) - ref.astype(int))
+        frac = (diff > 0).mean()
+        assert diff.max() <= 1, (dm, diff.max())
+        assert frac < 1e-3, (dm, frac)
+
+
+# ------------------------------------------------- incoherent dedispersion
+def test_incoherent_dedispersion_exact(cuda, oracle):
+    from skyweaver_b200 import stages, synthetic
+    g = synthetic.rng(41)
+    F, B, ts = 64, 64, 2
+    freqs = synthetic.channel_frequencies(580e6, 32e6, F)
+    dms = np.array([0, 10, 20, 30, 40], np.float32)
+    tsamp = 16 / (32e6 / F)
+    delays, maxd = oracle.idd_delays(freqs, dms, tsamp)
+    T = maxd + 64 * ts
+    tfb = g.integers(-128, 128, size=(T, F, B), dtype=np.int8)
+    sf = np.float32(math.sqrt(F * ts))
+    ref = oracle.idd(tfb, delays, maxd, ts, sf)
+    got = stages.incoherent_dedisperse(_dev(cuda, tfb), _dev(cuda, delays), maxd, ts, float(sf))
+    assert np.array_equal(_np(got), ref)
+
+
+def test_incoherent_dedispersion_ones(cuda, oracle):
+    """IncoherentDedisperserTester.cu:96-126: all-ones input -> sqrt(F*ts)."""
+    from skyweaver_b200 import stages, synthetic
+    F, B, ts = 64, 32, 2
+    freqs = synthetic.channel_frequencies(580e6, 32e6, F)
+    dms = np.array([0, 10, 20, 30, 40], np.float32)
+    delays, maxd = oracle.idd_delays(freqs, dms, 16 / (32e6 / F))
+    T = 3 * maxd
+    T -= (T - maxd) % ts
+    tfb = np.ones((T, F, B), np.int8)
+    got = _np(stages.incoherent_dedisperse(_dev(cuda, tfb), _dev(cuda, delays), maxd, ts,
+                                           float(np.float32(math.sqrt(F * ts)))))
+    assert got.shape == ((T - maxd) // ts, 5, B)
+    assert np.all(got == int(math.sqrt(F * ts)))
