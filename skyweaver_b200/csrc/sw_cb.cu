@@ -199,14 +199,68 @@ __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::aft
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
-// Stokes from the exact beam voltages, reference op order (beamformer_utils.cuh:125-140)
-__device__ __forceinline__ float stokes_f(int stokes, float r0, float i0, float r1, float i1)
+// ------------------------------------------------- exact packed arithmetic
+// Pairs of IEEE single operations (.rn, never contracted into an FMA), so
+// each element is rounded exactly like the reference's scalar host code.
+__device__ __forceinline__ uint64_t pack2(float lo, float hi)
 {
-    switch(stokes) {
-    case 0: return fadd(fadd(fmul(r0, r0), fmul(i0, i0)), fadd(fmul(r1, r1), fmul(i1, i1)));
-    case 1: return fsub(fadd(fmul(r0, r0), fmul(i0, i0)), fadd(fmul(r1, r1), fmul(i1, i1)));
-    case 2: return fmul(2.0f, fsub(fmul(r0, r1), fmul(i0, -i1)));
-    default: return fmul(2.0f, fadd(fmul(r0, -i1), fmul(i0, r1)));
+    uint64_t r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void unpack2(uint64_t v, float& lo, float& hi)
+{
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ uint64_t mul2(uint64_t a, uint64_t b)
+{
+    uint64_t d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b)
+{
+    uint64_t d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ uint64_t sub2(uint64_t a, uint64_t b)
+{
+    uint64_t d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+
+// Exact int32 -> float for |v| < 2^22 (beam voltages are below 2^21 for up
+// to 64 antennas): 1.5*2^23 + v is exactly representable, so building its
+// bit pattern with an integer add and subtracting 1.5*2^23 in float is exact
+// and avoids the low-throughput I2F conversion.
+constexpr uint32_t kMagicBits = 0x4B400000u;  // 12582912.0f
+__device__ __forceinline__ uint64_t to_float2(uint32_t a, uint32_t b)
+{
+    const uint64_t m = pack2(__uint_as_float(kMagicBits + a), __uint_as_float(kMagicBits + b));
+    return sub2(m, pack2(12582912.0f, 12582912.0f));
+}
+
+// Stokes of one sample from the exact beam voltages (p0 = r0 + i i0,
+// p1 = r1 + i i1) with the reference's operation order
+// (beamformer_utils.cuh:125-140: cuCmagf, cuCmulf with cuConjf).
+template <int STOKES>
+__device__ __forceinline__ float stokes_exact(uint32_t r0, uint32_t r1, uint32_t i0, uint32_t i1)
+{
+    float lo, hi;
+    if constexpr(STOKES <= 1) {
+        const uint64_t re = to_float2(r0, r1), im = to_float2(i0, i1);
+        unpack2(add2(mul2(re, re), mul2(im, im)), lo, hi);  // (|p0|^2, |p1|^2)
+        return STOKES == 0 ? fadd(lo, hi) : fsub(lo, hi);
+    } else if constexpr(STOKES == 2) {
+        // 2*Re(p0 conj p1) = 2*(r0 r1 - i0 (-i1))
+        unpack2(mul2(to_float2(r0, i0), to_float2(r1, i1)), lo, hi);
+        return fmul(2.0f, fadd(lo, hi));
+    } else {
+        // 2*Im(p0 conj p1) = 2*(r0 (-i1) + i0 r1)
+        unpack2(mul2(to_float2(i0, r0), to_float2(r1, i1)), lo, hi);
+        return fmul(2.0f, fsub(lo, hi));
     }
 }
 
@@ -231,6 +285,7 @@ __device__ __forceinline__ Item decode(const Params& P, int item)
     return it;
 }
 
+template <int TS, int STOKES>
 __global__ void __launch_bounds__(kThreads, 1)
 cb_kernel(const __grid_constant__ Params P)
 {
@@ -342,7 +397,7 @@ cb_kernel(const __grid_constant__ Params P)
         const int q = warp & 3;          // TMEM lane quarter of this warp
         const int h = (warp - 2) >> 2;   // which half of the tile's samples
         const int F = P.nchans;
-        const int nout = P.nsamples / P.tscrunch;
+        const int nout = P.nsamples / TS;
         int ab = 0;
         uint32_t aph = 0;
         for(int item = blockIdx.x; item < P.nitems && !*s_abort; item += gridDim.x) {
@@ -359,8 +414,8 @@ cb_kernel(const __grid_constant__ Params P)
             for(int tile = tile0; tile < tile1; ++tile) {
                 if(!mbar_wait(&acc_full[ab], aph, s_abort, deadline, P.err)) { ok = false; break; }
                 fence_after();
-                float power = 0.0f;
-                int count = 0;
+                float power = 0.0f;  // carried across the two groups when TS == 32
+#pragma unroll
                 for(int g = 0; g < 2; ++g) {
                     const int col = ab * 256 + h * 32 + g * 16;
                     const uint32_t ta = tmem + ((uint32_t)(q * 32) << 16) + col;
@@ -371,33 +426,32 @@ cb_kernel(const __grid_constant__ Params P)
                     SW_TMEM_LD16(ta + 192, i1);
                     tmem_wait_ld();
                     const int tbase = tile * kTileT + h * 32 + g * 16;
-#pragma unroll
-                    for(int t = 0; t < 16; ++t) {
-                        const float fr0 = __int2float_rn((int)r0[t]);
-                        const float fi0 = __int2float_rn((int)i0[t]);
-                        const float fr1 = __int2float_rn((int)r1[t]);
-                        const float fi1 = __int2float_rn((int)i1[t]);
-                        if(P.debug && valid) {
+                    if(P.debug != nullptr && valid) {
+                        int2* dbg = reinterpret_cast<int2*>(P.debug);
+                        for(int t = 0; t < 16; ++t) {
                             const size_t base_t = (size_t)it.f * P.nsamples + tbase + t;
-                            int2* dbg = reinterpret_cast<int2*>(P.debug);
                             dbg[(base_t * 2 + 0) * P.nbeams + b] = make_int2((int)r0[t], (int)i0[t]);
                             dbg[(base_t * 2 + 1) * P.nbeams + b] = make_int2((int)r1[t], (int)i1[t]);
                         }
-                        power = fadd(power, stokes_f(P.stokes, fr0, fi0, fr1, fi1));
-                        if(++count == P.tscrunch) {
-                            const int to = (tbase + t) / P.tscrunch;
+                    }
+#pragma unroll
+                    for(int t = 0; t < 16; ++t) {
+                        power = fadd(power, stokes_exact<STOKES>(r0[t], r1[t], i0[t], i1[t]));
+                        constexpr bool kWide = TS > 16;
+                        const bool emit = kWide ? (t == 15 && g == 1) : ((t + 1) % TS == 0);
+                        if(emit) {
+                            const int to = (tbase + t) / TS;
                             float v;
                             if(P.ib_subtract) {
                                 const float ib = pr.ib_raw[((size_t)bs * nout + to) * F + it.f];
                                 v = rintf(fdiv(fsub(power, fmul(ib, 16129.0f)), scale));
-                            } else if(P.stokes == 0) {
+                            } else if(STOKES == 0) {
                                 v = rintf(fdiv(fsub(power, offs), scale));
                             } else {
                                 v = rintf(fdiv(power, scale));
                             }
                             if(valid) pr.out[((size_t)to * F + it.f) * P.nbeams + b] = clamp_i8(v);
                             power = 0.0f;
-                            count = 0;
                         }
                     }
                 }
@@ -477,6 +531,16 @@ int make_wmap(CUtensorMap* map, const void* w, const sw_cb_shape& s)
     return SW_OK;
 }
 
+// Kernel parameter block of the launch being prepared on this host thread
+// (~6 KB, kept off the stack; copied into the launch).
+Params& launch_params()
+{
+    static thread_local Params P;
+    return P;
+}
+
+int dispatch_ts(int ts, int stokes, int grid, size_t smem, cudaStream_t stream);
+
 size_t smem_bytes(int kbytes)
 {
     return 1024 + (size_t)kWStages * 2 * kM * kbytes + (size_t)kVStages * 2 * kbytes * kTileT +
@@ -516,7 +580,7 @@ int launch(const sw_cb_shape* s, const sw_cb_problem* probs, int nprob,
     SW_REQUIRE(s->nbeams > 0 && s->nchans > 0, "CoherentBeamformer: empty shape");
     SW_REQUIRE(s->row_stride <= 0x7fffffffULL, "CoherentBeamformer: row stride too large");
 
-    static thread_local Params P;  // ~6 KB, kept off the stack
+    Params& P = launch_params();
     memset(&P, 0, sizeof(P));
     const void* dms[kMaxDm];
     int ndm = 0, item = 0;
@@ -574,12 +638,41 @@ int launch(const sw_cb_shape* s, const sw_cb_problem* probs, int nprob,
     P.timeout_ns = 5ull * 1000 * 1000 * 1000;                         // 5 s
 
     const size_t smem = smem_bytes(P.kbytes);
-    SW_CUDA_CHECK(cudaFuncSetAttribute(cb_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem));
     const int grid = P.nitems < num_sms() ? P.nitems : num_sms();
-    cb_kernel<<<grid, kThreads, smem, stream>>>(P);
+    return dispatch_ts(s->tscrunch, s->stokes, grid, smem, stream);
+}
+
+template <int TS, int STOKES>
+int launch_variant(int grid, size_t smem, cudaStream_t stream)
+{
+    SW_CUDA_CHECK(cudaFuncSetAttribute(cb_kernel<TS, STOKES>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    cb_kernel<TS, STOKES><<<grid, kThreads, smem, stream>>>(launch_params());
     SW_LAUNCH_CHECK();
     return SW_OK;
+}
+
+template <int TS>
+int dispatch_stokes(int stokes, int grid, size_t smem, cudaStream_t stream)
+{
+    switch(stokes) {
+    case 0: return launch_variant<TS, 0>(grid, smem, stream);
+    case 1: return launch_variant<TS, 1>(grid, smem, stream);
+    case 2: return launch_variant<TS, 2>(grid, smem, stream);
+    default: return launch_variant<TS, 3>(grid, smem, stream);
+    }
+}
+
+int dispatch_ts(int ts, int stokes, int grid, size_t smem, cudaStream_t stream)
+{
+    switch(ts) {
+    case 1: return dispatch_stokes<1>(stokes, grid, smem, stream);
+    case 2: return dispatch_stokes<2>(stokes, grid, smem, stream);
+    case 4: return dispatch_stokes<4>(stokes, grid, smem, stream);
+    case 8: return dispatch_stokes<8>(stokes, grid, smem, stream);
+    case 16: return dispatch_stokes<16>(stokes, grid, smem, stream);
+    default: return dispatch_stokes<32>(stokes, grid, smem, stream);
+    }
 }
 
 }  // namespace cb

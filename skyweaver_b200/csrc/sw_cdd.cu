@@ -266,8 +266,52 @@ __device__ __forceinline__ void fwd_pass(c32* buf, const c32* tw_s, int G, int s
     }
 }
 
+__device__ __forceinline__ uint32_t smem_addr(const void* p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Stage the int8 window of one work item (re row then im row, N bytes each)
+// into shared memory: asynchronously with 16-byte cp.async (zero-filled past
+// the end of the rows) when the rows and segment starts are 16-byte aligned,
+// otherwise with plain byte copies.
+template <int N, int NT>
+__device__ __forceinline__ void stage_input(uint8_t* st, const Args& A, int item, int L,
+                                            bool aligned)
+{
+    const int stream = item / A.nseg;
+    const int seg    = item - stream * A.nseg;
+    const uint8_t* row_re = A.in + (size_t)stream * 2 * A.row_stride;
+    const uint8_t* row_im = row_re + A.row_stride;
+    const int start = seg * L;
+    const int avail = A.overlap + A.nsamples;
+    if(aligned) {
+        constexpr int kChunks = N / 16;
+        for(int c = threadIdx.x; c < 2 * kChunks; c += NT) {
+            const int plane = c >= kChunks;
+            const int k     = (c - plane * kChunks) * 16;
+            const int left  = avail - (start + k);
+            const int bytes = left <= 0 ? 0 : (left >= 16 ? 16 : left);
+            const uint8_t* src = bytes > 0 ? (plane ? row_im : row_re) + start + k : row_re;
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(
+                             smem_addr(st + plane * N + k)),
+                         "l"(src), "r"(bytes)
+                         : "memory");
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    } else {
+        for(int i = threadIdx.x; i < N; i += NT) {
+            const int idx = start + i;
+            st[i]     = idx < avail ? row_re[idx] : 0;
+            st[N + i] = idx < avail ? row_im[idx] : 0;
+        }
+    }
+}
+
+// at least two resident CTAs per SM below N = 8192 (latency hiding across
+// the per-pass barriers); N = 8192 needs 512 threads and fits one.
 template <int LOGN>
-__global__ void __launch_bounds__((1 << LOGN) / 16)
+__global__ void __launch_bounds__((1 << LOGN) / 16, LOGN >= 13 ? 1 : (LOGN == 12 ? 2 : 4))
 cdd_kernel(const __grid_constant__ Args A)
 {
     constexpr int N  = 1 << LOGN;
@@ -278,23 +322,25 @@ cdd_kernel(const __grid_constant__ Args A)
     extern __shared__ __align__(16) uint8_t smem[];
     c32* buf  = reinterpret_cast<c32*>(smem);
     c32* tw_s = buf + pad(N) + 16;
+    uint8_t* stage = reinterpret_cast<uint8_t*>(tw_s + ((P.tw_total + 1) & ~1));
     for(int i = threadIdx.x; i < P.tw_total; i += NT) tw_s[i] = A.tw[i];
-    __syncthreads();
 
     const int L = N - A.overlap;
     const int half = A.overlap / 2;
     const float inv_n = 1.0f / (float)N;  // exact (power of two)
     const int nitems = A.nstreams * A.nseg;
+    const bool aligned = (A.row_stride % 16 == 0) && (L % 16 == 0) &&
+                         ((reinterpret_cast<uintptr_t>(A.in) & 15) == 0);
+    if(blockIdx.x < nitems) stage_input<N, NT>(stage, A, blockIdx.x, L, aligned);
     for(int item = blockIdx.x; item < nitems; item += gridDim.x) {
         const int stream = item / A.nseg;
         const int seg    = item - stream * A.nseg;
         const int f      = stream / A.npa;
-        const uint8_t* row_re = A.in + (size_t)stream * 2 * A.row_stride;
-        const uint8_t* row_im = row_re + A.row_stride;
-        const int start = seg * L;                 // first input sample of the window
-        const int avail = A.overlap + A.nsamples;  // history + gulp
+        const int start  = seg * L;  // first input sample of the window
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        __syncthreads();
 
-        // ---- forward pass 0 (radix R0, span N) straight from global int8
+        // ---- forward pass 0 (radix R0, span N) from the staged int8 window
         {
             constexpr int s0 = N / R0;
 #pragma unroll
@@ -303,9 +349,8 @@ cdd_kernel(const __grid_constant__ Args A)
                 c32 x[R0];
 #pragma unroll
                 for(int r = 0; r < R0; ++r) {
-                    const int idx = start + j + r * s0;
-                    x[r] = idx < avail ? c32{(float)(int8_t)row_re[idx], (float)(int8_t)row_im[idx]}
-                                       : c32{0.0f, 0.0f};
+                    const int i = j + r * s0;
+                    x[r] = c32{(float)(int8_t)stage[i], (float)(int8_t)stage[N + i]};
                 }
                 dft<R0, false>(x);
 #pragma unroll
@@ -315,6 +360,10 @@ cdd_kernel(const __grid_constant__ Args A)
             }
         }
         __syncthreads();
+        // the staging buffer is free: fetch the next work item's window now so
+        // that its global-memory latency hides behind this item's transforms
+        if(item + (int)gridDim.x < nitems)
+            stage_input<N, NT>(stage, A, item + gridDim.x, L, aligned);
         // ---- forward radix-16 passes except the last
 #pragma unroll
         for(int p = 1; p < P.npass - 1; ++p) {
@@ -326,13 +375,26 @@ cdd_kernel(const __grid_constant__ Args A)
 #pragma unroll
         for(int r = 0; r < 16; ++r) spec[r] = buf[pad(threadIdx.x * 16 + r)];
         dft16<false>(spec);
+
+        const size_t chirp_stride = (size_t)(A.nstreams / A.npa) * N;  // per DM
+        const float4* chp = reinterpret_cast<const float4*>(A.chirp + (size_t)f * N + threadIdx.x * 16);
+        float4 chn[8];
+#pragma unroll
+        for(int k = 0; k < 8; ++k) chn[k] = chp[k];
         __syncthreads();
 
         for(int d = 0; d < A.ndms; ++d) {
-            const c32* ch = A.chirp + ((size_t)d * (A.nstreams / A.npa) + f) * N + threadIdx.x * 16;
             c32 y[16];
 #pragma unroll
-            for(int q = 0; q < 16; ++q) y[q] = cmul(spec[q], ch[q]);
+            for(int k = 0; k < 8; ++k) {
+                y[2 * k]     = cmul(spec[2 * k], c32{chn[k].x, chn[k].y});
+                y[2 * k + 1] = cmul(spec[2 * k + 1], c32{chn[k].z, chn[k].w});
+            }
+            if(d + 1 < A.ndms) {  // next DM's chirp, in flight during this inverse
+                const float4* nxt = chp + (size_t)(d + 1) * chirp_stride / 2;
+#pragma unroll
+                for(int k = 0; k < 8; ++k) chn[k] = nxt[k];
+            }
             dft16<true>(y);
 #pragma unroll
             for(int r = 0; r < 16; ++r) buf[pad(threadIdx.x * 16 + r)] = y[r];
@@ -370,6 +432,7 @@ cdd_kernel(const __grid_constant__ Args A)
             __syncthreads();
         }
     }
+    asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
 // ------------------------------------------------------------- setup
@@ -422,7 +485,7 @@ int launch_logn(const Args& a, cudaStream_t stream)
 {
     constexpr int N = 1 << LOGN;
     constexpr Plan P = make_plan(LOGN);
-    const size_t smem = (size_t)(pad(N) + 16 + P.tw_total) * sizeof(c32);
+    const size_t smem = (size_t)(pad(N) + 16 + ((P.tw_total + 1) & ~1)) * sizeof(c32) + 2 * N;
     SW_CUDA_CHECK(cudaFuncSetAttribute(cdd_kernel<LOGN>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int dev = 0, nsm = 148, per_sm = 1;

@@ -191,6 +191,8 @@ class CoherentDedisperser:
     def dedisperse(self, fpact_ext, nsamples, outs=None, stream=None):
         """fpact_ext rows hold `overlap` history samples then the gulp."""
         F, P, A, _, stride = fpact_ext.shape
+        if F != self.nchans:
+            raise ValueError(f"voltages have {F} channels but the chirp tables {self.nchans}")
         nd = len(self.dms)
         if outs is None:
             outs = [torch.empty((F, P, A, 2, nsamples), dtype=torch.int8,

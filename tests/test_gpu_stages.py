@@ -251,7 +251,9 @@ def test_coherent_dedispersion_golden_vector(cuda):
     tsamp = 4096 / 856e6
     overlap = math.ceil(stages.dm_delay(856e6, 856e6 + 856e6 / 4096, 1000.0) / tsamp)
     assert overlap == 578
-    cdd = stages.CoherentDedisperser(64, 64, 1024, overlap, 856e6, 13.375e6, [0.0, 1000.0])
+    # channel 0 of the reference's 64-channel, 13.375 MHz configuration: a
+    # one-channel table with the same coarse channel width and centre
+    cdd = stages.CoherentDedisperser(1, 64, 1024, overlap, 856e6, 13.375e6 / 64, [0.0, 1000.0])
     fp = _dev(cuda, inp.transpose(1, 2, 3, 0)[None].copy())   # [1][P][A][C][1024]
     outs = cdd.dedisperse(fp, 1024 - overlap)
     got = _np(outs[1])[0].transpose(3, 0, 1, 2)                # [446][P][A][C]
