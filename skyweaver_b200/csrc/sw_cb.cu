@@ -42,8 +42,12 @@ constexpr int kWStages     = 2;
 constexpr int kTilesPerItem = 16;  // 1024 samples of one channel per item
 constexpr int kMaxDm       = 16;
 constexpr int kMaxProblems = 96;
-constexpr int kEpiWarps    = 8;
-constexpr int kThreads     = 32 * (2 + kEpiWarps);
+// Epilogue warps: four per TMEM lane quarter, each owning 16 samples of a
+// tile; tscrunch 32 needs 32 samples per warp, so two per quarter.
+template <int TS>
+constexpr int epi_warps() { return TS > 16 ? 8 : 16; }
+template <int TS>
+constexpr int cb_threads() { return 32 * (2 + epi_warps<TS>()); }
 constexpr int kTmemCols    = 512;
 
 struct Problem {
@@ -199,6 +203,28 @@ __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::aft
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
+#define SW_TMEM_LD8(taddr, r)                                                              \
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"    \
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),  \
+                   "=r"(r[6]), "=r"(r[7])                                                   \
+                 : "r"(taddr))
+
+#define SW_TMEM_ST8(taddr, r)                                                              \
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};"   \
+                 ::"r"(taddr), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]),         \
+                 "r"(r[5]), "r"(r[6]), "r"(r[7])                                              \
+                 : "memory")
+
+#define SW_TMEM_ST16(taddr, r)                                                              \
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x16.b32 "                                  \
+                 "[%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(taddr), \
+                 "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]),  \
+                 "r"(r[7]), "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]),          \
+                 "r"(r[13]), "r"(r[14]), "r"(r[15])                                            \
+                 : "memory")
+
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
 // ------------------------------------------------- exact packed arithmetic
 // Pairs of IEEE single operations (.rn, never contracted into an FMA), so
 // each element is rounded exactly like the reference's scalar host code.
@@ -231,36 +257,56 @@ __device__ __forceinline__ uint64_t sub2(uint64_t a, uint64_t b)
     return d;
 }
 
-// Exact int32 -> float for |v| < 2^22 (beam voltages are below 2^21 for up
-// to 64 antennas): 1.5*2^23 + v is exactly representable, so building its
-// bit pattern with an integer add and subtracting 1.5*2^23 in float is exact
-// and avoids the low-throughput I2F conversion.
+// Exact int32 -> float without the low-throughput I2F conversion: every
+// accumulator element starts at the bit pattern of 1.5*2^23 (0x4B400000)
+// and the MMAs add the int32 sum v to it.  For |v| < 2^22 (beam voltages
+// stay below 2^21 for up to 64 antennas) the result is the float
+// 1.5*2^23 + v exactly, and subtracting 1.5*2^23 in float recovers v.
 constexpr uint32_t kMagicBits = 0x4B400000u;  // 12582912.0f
-__device__ __forceinline__ uint64_t to_float2(uint32_t a, uint32_t b)
+
+__device__ __forceinline__ uint64_t pair_f(const uint32_t* w, int t)
 {
-    const uint64_t m = pack2(__uint_as_float(kMagicBits + a), __uint_as_float(kMagicBits + b));
-    return sub2(m, pack2(12582912.0f, 12582912.0f));
+    return sub2(pack2(__uint_as_float(w[t]), __uint_as_float(w[t + 1])),
+                pack2(12582912.0f, 12582912.0f));
 }
 
-// Stokes of one sample from the exact beam voltages (p0 = r0 + i i0,
-// p1 = r1 + i i1) with the reference's operation order
-// (beamformer_utils.cuh:125-140: cuCmagf, cuCmulf with cuConjf).
-template <int STOKES>
-__device__ __forceinline__ float stokes_exact(uint32_t r0, uint32_t r1, uint32_t i0, uint32_t i1)
+// Stokes of 16 consecutive samples from the exact beam voltages
+// (p0 = r0 + i i0, p1 = r1 + i i1) with the reference's operation order
+// (beamformer_utils.cuh:125-140: cuCmagf, cuCmulf with cuConjf).  Products
+// are computed two samples at a time with packed multiplies; every sum is a
+// scalar add.rn.f32 so that nothing is contracted into an FMA.
+template <int STOKES, int L>
+__device__ __forceinline__ void stokes_n(const uint32_t* r0, const uint32_t* r1,
+                                         const uint32_t* i0, const uint32_t* i1, float* st)
 {
-    float lo, hi;
-    if constexpr(STOKES <= 1) {
-        const uint64_t re = to_float2(r0, r1), im = to_float2(i0, i1);
-        unpack2(add2(mul2(re, re), mul2(im, im)), lo, hi);  // (|p0|^2, |p1|^2)
-        return STOKES == 0 ? fadd(lo, hi) : fsub(lo, hi);
-    } else if constexpr(STOKES == 2) {
-        // 2*Re(p0 conj p1) = 2*(r0 r1 - i0 (-i1))
-        unpack2(mul2(to_float2(r0, i0), to_float2(r1, i1)), lo, hi);
-        return fmul(2.0f, fadd(lo, hi));
-    } else {
-        // 2*Im(p0 conj p1) = 2*(r0 (-i1) + i0 r1)
-        unpack2(mul2(to_float2(i0, r0), to_float2(r1, i1)), lo, hi);
-        return fmul(2.0f, fsub(lo, hi));
+#pragma unroll
+    for(int t = 0; t < L; t += 2) {
+        const uint64_t R0 = pair_f(r0, t), R1 = pair_f(r1, t);
+        const uint64_t I0 = pair_f(i0, t), I1 = pair_f(i1, t);
+        float a0, a1, b0, b1;
+        if constexpr(STOKES <= 1) {
+            float c0, c1, d0, d1;
+            unpack2(mul2(R0, R0), a0, a1);  // re0^2
+            unpack2(mul2(I0, I0), b0, b1);  // im0^2
+            unpack2(mul2(R1, R1), c0, c1);  // re1^2
+            unpack2(mul2(I1, I1), d0, d1);  // im1^2
+            const float e00 = fadd(a0, b0), e10 = fadd(c0, d0);  // |p0|^2, |p1|^2
+            const float e01 = fadd(a1, b1), e11 = fadd(c1, d1);
+            st[t]     = STOKES == 0 ? fadd(e00, e10) : fsub(e00, e10);
+            st[t + 1] = STOKES == 0 ? fadd(e01, e11) : fsub(e01, e11);
+        } else if constexpr(STOKES == 2) {
+            // 2*Re(p0 conj p1) = 2*(r0 r1 - i0 (-i1)) = 2*(r0 r1 + i0 i1)
+            unpack2(mul2(R0, R1), a0, a1);
+            unpack2(mul2(I0, I1), b0, b1);
+            st[t]     = fmul(2.0f, fadd(a0, b0));
+            st[t + 1] = fmul(2.0f, fadd(a1, b1));
+        } else {
+            // 2*Im(p0 conj p1) = 2*(r0 (-i1) + i0 r1) = 2*(i0 r1 - r0 i1)
+            unpack2(mul2(I0, R1), a0, a1);
+            unpack2(mul2(R0, I1), b0, b1);
+            st[t]     = fmul(2.0f, fsub(a0, b0));
+            st[t + 1] = fmul(2.0f, fsub(a1, b1));
+        }
     }
 }
 
@@ -286,7 +332,7 @@ __device__ __forceinline__ Item decode(const Params& P, int item)
 }
 
 template <int TS, int STOKES>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(cb_threads<TS>(), 1)
 cb_kernel(const __grid_constant__ Params P)
 {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -314,7 +360,7 @@ cb_kernel(const __grid_constant__ Params P)
     if(threadIdx.x == 0) {
         for(int i = 0; i < kVStages; ++i) { mbar_init(&v_full[i], 1); mbar_init(&v_empty[i], 1); }
         for(int i = 0; i < kWStages; ++i) { mbar_init(&w_full[i], 1); mbar_init(&w_empty[i], 1); }
-        for(int i = 0; i < 2; ++i) { mbar_init(&acc_full[i], 1); mbar_init(&acc_empty[i], kEpiWarps); }
+        for(int i = 0; i < 2; ++i) { mbar_init(&acc_full[i], 1); mbar_init(&acc_empty[i], epi_warps<TS>()); }
         *s_abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -370,7 +416,9 @@ cb_kernel(const __grid_constant__ Params P)
                 bool ok = true;
                 for(int tile = tile0; tile < tile1; ++tile) {
                     if(!mbar_wait(&v_full[vs], vph, s_abort, deadline, P.err)) { ok = false; break; }
-                    if(!mbar_wait(&acc_empty[ab], aph ^ 1, s_abort, deadline, P.err)) { ok = false; break; }
+                    // phase 0 of acc_empty is completed by the epilogue's
+                    // initial fill of both buffers with the magic constant
+                    if(!mbar_wait(&acc_empty[ab], aph, s_abort, deadline, P.err)) { ok = false; break; }
                     fence_after();
                     const uint32_t vb = smem_u32(vbuf + vs * vtile);
                     const uint32_t d_re = tmem + ab * 256;
@@ -379,8 +427,10 @@ cb_kernel(const __grid_constant__ Params P)
                         const uint64_t adr = make_desc(wa + ks * 32, 1, P.w_sbo16, P.w_layout);
                         const uint64_t adi = make_desc(wa + wtile + ks * 32, 1, P.w_sbo16, P.w_layout);
                         const uint64_t bd  = make_desc(vb + ks * 2048, P.v_lbo16, 32, 4 /*SW64*/);
-                        mma_i8(d_re, adr, bd, P.idesc, ks > 0);
-                        mma_i8(d_im, adi, bd, P.idesc, ks > 0);
+                        // always accumulate: the buffer holds 0x4B400000
+                        // per element, so D = 1.5*2^23 (as float bits) + sum
+                        mma_i8(d_re, adr, bd, P.idesc, 1);
+                        mma_i8(d_im, adi, bd, P.idesc, 1);
                     }
                     mma_commit(&v_empty[vs]);
                     mma_commit(&acc_full[ab]);
@@ -394,10 +444,29 @@ cb_kernel(const __grid_constant__ Params P)
         }
     } else {
         // ------------------------------------------------------ epilogue
+        constexpr int kSlice  = TS > 16 ? 32 : 16;   // samples per warp per tile
+        constexpr int kGroups = kSlice / 8;          // x8 column groups per warp
         const int q = warp & 3;          // TMEM lane quarter of this warp
-        const int h = (warp - 2) >> 2;   // which half of the tile's samples
+        const int h = (warp - 2) >> 2;   // which slice of the tile's 64 samples
         const int F = P.nchans;
         const int nout = P.nsamples / TS;
+        const uint32_t lane_base = tmem + ((uint32_t)(q * 32) << 16);
+        uint32_t magic[8];
+#pragma unroll
+        for(int k = 0; k < 8; ++k) magic[k] = kMagicBits;
+        // fill this warp's columns of both accumulator buffers with the magic
+        // constant, then release both buffers to the MMA warp (phase 0)
+#pragma unroll
+        for(int buf = 0; buf < 2; ++buf)
+#pragma unroll
+            for(int g = 0; g < kGroups; ++g)
+#pragma unroll
+                for(int sec = 0; sec < 4; ++sec)
+                    SW_TMEM_ST8(lane_base + buf * 256 + sec * 64 + h * kSlice + g * 8, magic);
+        tmem_wait_st();
+        fence_before();
+        __syncwarp();
+        if(lane == 0) { mbar_arrive(&acc_empty[0]); mbar_arrive(&acc_empty[1]); }
         int ab = 0;
         uint32_t aph = 0;
         for(int item = blockIdx.x; item < P.nitems && !*s_abort; item += gridDim.x) {
@@ -414,31 +483,39 @@ cb_kernel(const __grid_constant__ Params P)
             for(int tile = tile0; tile < tile1; ++tile) {
                 if(!mbar_wait(&acc_full[ab], aph, s_abort, deadline, P.err)) { ok = false; break; }
                 fence_after();
-                float power = 0.0f;  // carried across the two groups when TS == 32
+                float power = 0.0f;  // carried across groups while tscrunch > 8
 #pragma unroll
-                for(int g = 0; g < 2; ++g) {
-                    const int col = ab * 256 + h * 32 + g * 16;
-                    const uint32_t ta = tmem + ((uint32_t)(q * 32) << 16) + col;
-                    uint32_t r0[16], r1[16], i0[16], i1[16];
-                    SW_TMEM_LD16(ta, r0);
-                    SW_TMEM_LD16(ta + 64, r1);
-                    SW_TMEM_LD16(ta + 128, i0);
-                    SW_TMEM_LD16(ta + 192, i1);
+                for(int g = 0; g < kGroups; ++g) {
+                    const uint32_t ta = lane_base + ab * 256 + h * kSlice + g * 8;
+                    uint32_t r0[8], r1[8], i0[8], i1[8];
+                    SW_TMEM_LD8(ta, r0);
+                    SW_TMEM_LD8(ta + 64, r1);
+                    SW_TMEM_LD8(ta + 128, i0);
+                    SW_TMEM_LD8(ta + 192, i1);
                     tmem_wait_ld();
-                    const int tbase = tile * kTileT + h * 32 + g * 16;
+                    // re-arm these columns for the next tile that uses this buffer
+                    SW_TMEM_ST8(ta, magic);
+                    SW_TMEM_ST8(ta + 64, magic);
+                    SW_TMEM_ST8(ta + 128, magic);
+                    SW_TMEM_ST8(ta + 192, magic);
+                    const int tbase = tile * kTileT + h * kSlice + g * 8;
                     if(P.debug != nullptr && valid) {
                         int2* dbg = reinterpret_cast<int2*>(P.debug);
-                        for(int t = 0; t < 16; ++t) {
+                        for(int t = 0; t < 8; ++t) {
                             const size_t base_t = (size_t)it.f * P.nsamples + tbase + t;
-                            dbg[(base_t * 2 + 0) * P.nbeams + b] = make_int2((int)r0[t], (int)i0[t]);
-                            dbg[(base_t * 2 + 1) * P.nbeams + b] = make_int2((int)r1[t], (int)i1[t]);
+                            dbg[(base_t * 2 + 0) * P.nbeams + b] =
+                                make_int2((int)(r0[t] - kMagicBits), (int)(i0[t] - kMagicBits));
+                            dbg[(base_t * 2 + 1) * P.nbeams + b] =
+                                make_int2((int)(r1[t] - kMagicBits), (int)(i1[t] - kMagicBits));
                         }
                     }
+                    float st[8];
+                    stokes_n<STOKES, 8>(r0, r1, i0, i1, st);
 #pragma unroll
-                    for(int t = 0; t < 16; ++t) {
-                        power = fadd(power, stokes_exact<STOKES>(r0[t], r1[t], i0[t], i1[t]));
-                        constexpr bool kWide = TS > 16;
-                        const bool emit = kWide ? (t == 15 && g == 1) : ((t + 1) % TS == 0);
+                    for(int t = 0; t < 8; ++t) {
+                        power = fadd(power, st[t]);
+                        const int u = g * 8 + t;  // sample within this warp's slice
+                        const bool emit = ((u + 1) % TS) == 0;
                         if(emit) {
                             const int to = (tbase + t) / TS;
                             float v;
@@ -455,6 +532,7 @@ cb_kernel(const __grid_constant__ Params P)
                         }
                     }
                 }
+                tmem_wait_st();
                 fence_before();
                 __syncwarp();
                 if(lane == 0) mbar_arrive(&acc_empty[ab]);
@@ -647,7 +725,7 @@ int launch_variant(int grid, size_t smem, cudaStream_t stream)
 {
     SW_CUDA_CHECK(cudaFuncSetAttribute(cb_kernel<TS, STOKES>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    cb_kernel<TS, STOKES><<<grid, kThreads, smem, stream>>>(launch_params());
+    cb_kernel<TS, STOKES><<<grid, cb_threads<TS>(), smem, stream>>>(launch_params());
     SW_LAUNCH_CHECK();
     return SW_OK;
 }

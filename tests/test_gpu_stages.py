@@ -198,11 +198,23 @@ def test_coherent_beam_voltages_and_power_exact(cuda, oracle, A):
     assert np.array_equal(out, ref)       # int8 TFB identical to the CPU reference
 
 
+def _report(out, ref):
+    bad = np.argwhere(out != ref)
+    lines = [f"{len(bad)} of {out.size} differ"]
+    for idx in bad[:8]:
+        lines.append(f"  {tuple(idx)}: got {out[tuple(idx)]} want {ref[tuple(idx)]}")
+    return "\n".join(lines)
+
+
 @pytest.mark.parametrize("stokes", ["I", "Q", "U", "V"])
 @pytest.mark.parametrize("ib_sub", [True, False])
 def test_coherent_beam_stokes(cuda, oracle, stokes, ib_sub):
-    out, ref, _, _ = _cb_case(cuda, oracle, 64, 256, 3, 2, 4, stokes, ib_sub, seed=22)
-    assert np.array_equal(out, ref)
+    out, ref, dbg, volts = _cb_case(cuda, oracle, 64, 256, 3, 2, 4, stokes, ib_sub, seed=22)
+    assert np.array_equal(dbg, volts)
+    assert np.array_equal(out, ref), _report(out, ref)
+    # run-to-run determinism of the whole chain
+    out2, _, _, _ = _cb_case(cuda, oracle, 64, 256, 3, 2, 4, stokes, ib_sub, seed=22)
+    assert np.array_equal(out, out2), _report(out2, out)
 
 
 def test_coherent_beam_partial_block_and_tscrunch(cuda, oracle):
