@@ -109,6 +109,24 @@ int sw_statistics(const void* d_fpact, size_t row_stride, size_t sample_offset,
                   int nchans, int npol, int nant, int nsamples,
                   void* d_scratch, float* d_stats, sw_stream_t stream);
 
+/* No counterpart in the reference.  Same result as sw_statistics, for callers
+ * that cannot allocate device memory (a real-time ingest loop that must not
+ * take cudaMalloc's implicit device synchronisation, or a process whose
+ * device memory is owned by another component): the workspace is a
+ * file-scope device array of the library, so this call allocates nothing.
+ *   - at most 16384 (channel, pol, antenna) series; larger shapes return
+ *     SW_ERR_INVALID with a message, nothing is launched;
+ *   - the first call on each device looks up the array's device address
+ *     (cudaGetSymbolAddress with that device current); make that first call
+ *     before capturing any stream;
+ *   - every call shares the one array (it is cleared at the start of each
+ *     call): calls whose kernels overlap on the GPU, from any stream or
+ *     thread, race and give wrong statistics;
+ *   - every GPU that loads the library holds the 512 KiB array until exit. */
+int sw_statistics_noalloc(const void* d_fpact, size_t row_stride,
+                          size_t sample_offset, int nchans, int npol, int nant,
+                          int nsamples, float* d_stats, sw_stream_t stream);
+
 /* Replaces StatisticsCalculator::update_scalings
  * (cpp/skyweaver/StatisticsCalculator.cuh:96-97,
  *  cpp/skyweaver/src/StatisticsCalculator.cu:132-239), computed on the

@@ -12,6 +12,9 @@
 // on the device with the same IEEE single operations in the same order; its
 // outputs are indexed [beamset][chan] (the reference writes [chan] for every
 // beamset).
+#include <mutex>
+#include <vector>
+
 #include "sw_common.cuh"
 
 namespace swb {
@@ -165,11 +168,64 @@ int launch_statistics(const void* d_fpact, size_t row_stride,
     return SW_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free statistics.  Some callers cannot call cudaMalloc/cudaFree:
+// a real-time ingest loop where the implicit device synchronisation of an
+// allocation would stall the transfers and kernels already in flight, or a
+// host process whose device memory is owned up front by another component
+// (a ring-buffer manager, a memory pool) and gives this library no
+// allocation rights.  For them sw_statistics_noalloc keeps its workspace in
+// the file-scope array below, which every GPU that loads the library holds
+// until the process exits.
+constexpr int kNoAllocMaxSeries = 16384;  // channels x pols x antennas
+static __device__ __align__(256) long long g_stats_noalloc_sums[kNoAllocMaxSeries * 4];
+
+namespace {
+
+// Device address of g_stats_noalloc_sums on the current device.  The host
+// symbol is only a stand-in, so the address is looked up once per device
+// (with that device current) and cached.
+int noalloc_sums(long long** out)
+{
+    static std::mutex mu;
+    static std::vector<long long*> per_device;
+    int dev = -1;
+    SW_CUDA_CHECK(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    if((size_t)dev >= per_device.size()) per_device.resize(dev + 1, nullptr);
+    if(per_device[dev] == nullptr) {
+        void* p = nullptr;
+        SW_CUDA_CHECK(cudaGetSymbolAddress(&p, g_stats_noalloc_sums));
+        per_device[dev] = static_cast<long long*>(p);
+    }
+    *out = per_device[dev];
+    return SW_OK;
+}
+
+}  // namespace
+
 }  // namespace swb
 
 using namespace swb;
 
 extern "C" {
+
+int sw_statistics_noalloc(const void* d_fpact, size_t row_stride, size_t sample_offset,
+                          int nchans, int npol, int nant, int nsamples, float* d_stats,
+                          sw_stream_t stream)
+{
+    const long long nseries = (long long)nchans * npol * nant;
+    SW_REQUIRE(nseries > 0 && nseries <= kNoAllocMaxSeries,
+               "sw_statistics_noalloc: %lld (channel, pol, antenna) series exceed the "
+               "built-in workspace of %d; use sw_statistics with a caller workspace",
+               nseries, kNoAllocMaxSeries);
+    long long* sums = nullptr;
+    const int rc = noalloc_sums(&sums);
+    if(rc != SW_OK) return rc;
+    // launch_statistics clears the sums before accumulating into them
+    return launch_statistics(d_fpact, row_stride, sample_offset, nchans, npol, nant, nsamples,
+                             sums, d_stats, as_cuda(stream));
+}
 
 size_t sw_statistics_scratch_bytes(int nchans, int npol, int nant)
 {
