@@ -52,7 +52,9 @@ __host__ __device__ constexpr Plan make_plan(int logn)
         P.span[p]   = g;
         P.stride[p] = g / r;
         P.tw_off[p] = off;
-        if(P.stride[p] > 1) off += (r - 1) * P.stride[p];
+        // radix-16 tables hold twiddle pairs (w1,w2),(w3,w4),..,(w15,0) per j,
+        // read with one 16-byte load per pair; other radices hold w1..w(R-1)
+        if(P.stride[p] > 1) off += (r == 16 ? 16 : r - 1) * P.stride[p];
         g /= r;
         r = 16;
         ++p;
@@ -215,6 +217,24 @@ struct Args {
     size_t out_stride;
 };
 
+// Twiddles w[1..R-1] of butterfly column j for a pass with stride s.
+template <int R>
+__device__ __forceinline__ void load_tw(const c32* tw_s, int tw_off, int s, int j, c32* w)
+{
+    if constexpr(R == 16) {
+        const float4* p = reinterpret_cast<const float4*>(tw_s + tw_off);
+#pragma unroll
+        for(int k = 0; k < 8; ++k) {
+            const float4 v = p[k * s + j];
+            w[2 * k + 1] = c32{v.x, v.y};
+            if(k < 7) w[2 * k + 2] = c32{v.z, v.w};
+        }
+    } else {
+#pragma unroll
+        for(int q = 1; q < R; ++q) w[q] = tw_s[tw_off + (q - 1) * s + j];
+    }
+}
+
 // One radix-R pass of the inverse (DIT) on shared memory.
 template <int LOGN, int R>
 __device__ __forceinline__ void inv_pass(c32* buf, const c32* tw_s, int G, int s,
@@ -232,8 +252,12 @@ __device__ __forceinline__ void inv_pass(c32* buf, const c32* tw_s, int G, int s
 #pragma unroll
         for(int q = 0; q < R; ++q) z[q] = buf[pad(base + q * s)];
         if(s > 1) {
+{
+                c32 w[R];
+                load_tw<R>(tw_s, tw_off, s, j, w);
 #pragma unroll
-            for(int q = 1; q < R; ++q) z[q] = cmulc(z[q], tw_s[tw_off + (q - 1) * s + j]);
+                for(int q = 1; q < R; ++q) z[q] = cmulc(z[q], w[q]);
+            }
         }
         dft<R, true>(z);
 #pragma unroll
@@ -258,8 +282,12 @@ __device__ __forceinline__ void fwd_pass(c32* buf, const c32* tw_s, int G, int s
         for(int r = 0; r < R; ++r) x[r] = buf[pad(base + r * s)];
         dft<R, false>(x);
         if(s > 1) {
+{
+                c32 w[R];
+                load_tw<R>(tw_s, tw_off, s, j, w);
 #pragma unroll
-            for(int q = 1; q < R; ++q) x[q] = cmul(x[q], tw_s[tw_off + (q - 1) * s + j]);
+                for(int q = 1; q < R; ++q) x[q] = cmul(x[q], w[q]);
+            }
         }
 #pragma unroll
         for(int q = 0; q < R; ++q) buf[pad(base + q * s)] = x[q];
@@ -353,8 +381,12 @@ cdd_kernel(const __grid_constant__ Args A)
                     x[r] = c32{(float)(int8_t)stage[i], (float)(int8_t)stage[N + i]};
                 }
                 dft<R0, false>(x);
+{
+                    c32 w[R0];
+                    load_tw<R0>(tw_s, P.tw_off[0], s0, j, w);
 #pragma unroll
-                for(int q = 1; q < R0; ++q) x[q] = cmul(x[q], tw_s[P.tw_off[0] + (q - 1) * s0 + j]);
+                    for(int q = 1; q < R0; ++q) x[q] = cmul(x[q], w[q]);
+                }
 #pragma unroll
                 for(int q = 0; q < R0; ++q) buf[pad(j + q * s0)] = x[q];
             }
@@ -414,8 +446,12 @@ cdd_kernel(const __grid_constant__ Args A)
                 c32 z[R0];
 #pragma unroll
                 for(int q = 0; q < R0; ++q) z[q] = buf[pad(j + q * s0)];
+{
+                    c32 w[R0];
+                    load_tw<R0>(tw_s, P.tw_off[0], s0, j, w);
 #pragma unroll
-                for(int q = 1; q < R0; ++q) z[q] = cmulc(z[q], tw_s[P.tw_off[0] + (q - 1) * s0 + j]);
+                    for(int q = 1; q < R0; ++q) z[q] = cmulc(z[q], w[q]);
+                }
                 dft<R0, true>(z);
 #pragma unroll
                 for(int r = 0; r < R0; ++r) {
@@ -448,12 +484,21 @@ __global__ void twiddle_k(c32* tw, int logn)
     for(int p = 0; p < P.npass; ++p) {
         const int s = P.stride[p], R = P.radix[p], G = P.span[p];
         if(s <= 1) continue;
-        for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < (R - 1) * s;
+        const int entries = (R == 16 ? 16 : R - 1) * s;
+        for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < entries;
             i += gridDim.x * blockDim.x) {
-            const int q = i / s + 1, j = i % s;
-            double sn, cs;
+            int q, j;
+            if(R == 16) {  // c32 index i = 2*(k*s + j) + h holds w_(2k+1+h)
+                const int m = i >> 1, h = i & 1;
+                q = 2 * (m / s) + 1 + h;
+                j = m % s;
+            } else {
+                q = i / s + 1;
+                j = i % s;
+            }
+            double sn = 0.0, cs = 0.0;
             // exp(-2 pi i j q / G) in FP64
-            sincospi(-2.0 * (double)(j * q) / (double)G, &sn, &cs);
+            if(q < R) sincospi(-2.0 * (double)(j * q) / (double)G, &sn, &cs);
             tw[P.tw_off[p] + i] = c32{(float)cs, (float)sn};
         }
     }

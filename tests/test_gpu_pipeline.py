@@ -1,0 +1,91 @@
+"""End-to-end parity of the graph-captured BeamformerPipeline against the
+oracle chain over consecutive gulps (overlap-save history carried across
+gulps, scalings fixed from gulp 0 like BeamformerPipeline.cu:171-176).
+
+DM 0 must be bit-identical (its chirp is exactly 1, so dedispersion is an
+exact delay).  For a non-zero DM the FP32 FFT may move a dedispersed voltage
+by one LSB against the FP64 oracle, which can move a beam sample by one LSB:
+those are bounded in count below.
+"""
+import math
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(cuda, oracle, use_graph, grouped):
+    torch = cuda
+    from skyweaver_b200 import stages, synthetic
+    g = synthetic.rng(77)
+    A_in, A, F, B, T, ts = 13, 16, 4, 64, 4096, 4
+    chbw = 856e6 / 1024
+    centre, bw = 1284e6, F * chbw
+    dms = [0.0, 10.0]
+    mapping = np.zeros(B, np.int32)
+    mapping[40:] = 1
+    masks = np.ones((2, A), np.float32)
+    masks[:, A_in:] = 0
+    masks[1, :5] = 0
+    delays = synthetic.delay_model(g, B, A)
+    delays[..., 0] = masks[mapping]
+    pipe = stages.BeamformerPipeline(nantennas=A, input_nantennas=A_in, nchans=F, nbeams=B,
+                                     gulp_samples=T, tscrunch=ts, centre_frequency=centre,
+                                     bandwidth=bw, dms=dms, beamset_weights=masks,
+                                     beamset_mapping=mapping, use_graph=use_graph,
+                                     grouped=grouped)
+    epoch0, delay_epoch = 1.7e9, 1.7e9 - 3.0
+    pipe.set_delays(delays, delay_epoch)
+    fft_len, overlap = pipe.fft_plan()
+    freqs = synthetic.channel_frequencies(centre, bw, F)
+    low = float(np.float32(centre - bw / 2))
+    chirps = [oracle.chirp(F, fft_len, low, bw, d) for d in dms]
+    history = np.zeros((F, overlap, 2, A, 2), np.int8)
+    scl = None
+    results = []
+    for gulp in range(3):
+        taftp = synthetic.voltages_taftp(g, T // 256, A_in, F, sigma=10)
+        epoch = epoch0 + gulp * T / chbw
+        pipe.process_device(torch.from_numpy(taftp).cuda(), epoch)
+        ftpa = oracle.transpose(taftp, A)
+        stats_ref = oracle.statistics(ftpa)
+        out0 = pipe.outputs(0)
+        stats_gpu = pipe_stats(pipe, F, A)
+        np.testing.assert_allclose(stats_gpu, stats_ref, rtol=1e-5, atol=1e-6)
+        if scl is None:  # scalings come from gulp 0's statistics
+            scl = oracle.scalings(stats_gpu, masks, 2, ts, ts, 24.0)
+        w = oracle.weights(delays, freqs, epoch, delay_epoch)
+        ext = np.concatenate([history, ftpa], axis=1)
+        history = ext[:, -overlap:].copy() if overlap else history
+        for d, dm in enumerate(dms):
+            dd = oracle.cdd_ftpa(ext, T, chirps[d], overlap)
+            raw_ref, ib_ref = oracle.incoherent_beam(dd, ts, scl[3], scl[2], masks, 2)
+            cb_ref = oracle.coherent_beam(dd, w, ts, scl[1], scl[0], masks, mapping)
+            out = out0 if d == 0 else pipe.outputs(d)
+            results.append((dm, out, raw_ref, ib_ref, cb_ref))
+    pipe.close()
+    return results
+
+
+def pipe_stats(pipe, F, A):
+    import ctypes
+    from skyweaver_b200._lib import call
+    from skyweaver_b200.stages import _device_view
+    ptrs = [ctypes.c_void_p() for _ in range(4)]
+    call("sw_pipeline_outputs", pipe.h, 0, *[ctypes.byref(p) for p in ptrs])
+    n = F * 2 * A * 4
+    return _device_view(ptrs[3].value, n * 4).cpu().numpy().view(np.float32).reshape(F, 2, A, 4)
+
+
+@pytest.mark.parametrize("use_graph,grouped", [(True, True), (False, False)])
+def test_pipeline_matches_oracle_chain(cuda, oracle, use_graph, grouped):
+    for dm, out, raw_ref, ib_ref, cb_ref in _run(cuda, oracle, use_graph, grouped):
+        if dm == 0.0:
+            assert np.array_equal(out["ib_raw"], raw_ref)
+            assert np.array_equal(out["ib"], ib_ref)
+            assert np.array_equal(out["cb"], cb_ref)
+        else:
+            diff = np.abs(out["cb"].astype(int) - cb_ref.astype(int))
+            assert (diff > 0).mean() < 2e-3, (diff > 0).mean()
+            assert np.allclose(out["ib_raw"], raw_ref, rtol=1e-3)
