@@ -276,90 +276,36 @@ __device__ __forceinline__ uint64_t pair_f(const uint32_t* w, int t)
                 pack2(12582912.0f, 12582912.0f));
 }
 
-// Stokes of 16 consecutive samples from the exact beam voltages
+// Stokes of L consecutive samples from the exact beam voltages
 // (p0 = r0 + i i0, p1 = r1 + i i1) with the reference's operation order
-// (beamformer_utils.cuh:125-140: cuCmagf, cuCmulf with cuConjf).  Products
-// are computed two samples at a time with packed multiplies; every sum is a
-// scalar add.rn.f32 so that nothing is contracted into an FMA.
-#ifndef SW_CB_EPI
-#define SW_CB_EPI 0
-#endif
-__device__ __forceinline__ float magic_f(uint32_t w) { return fsub(__uint_as_float(w), 12582912.0f); }
-
+// (beamformer_utils.cuh:125-140: cuCmagf, cuCmulf with cuConjf), two samples
+// per packed instruction.  Products are fma(a, b, +0): one rounding exactly
+// like a multiply, and since an FMA result cannot be contracted into the
+// packed add that consumes it, every sum is also a single rounding.  (A
+// packed multiply feeding a packed add was measured to be contracted into an
+// FMA, which moved 1 in ~1e5 outputs by one LSB.)
 template <int STOKES, int L>
 __device__ __forceinline__ void stokes_n(const uint32_t* r0, const uint32_t* r1,
                                          const uint32_t* i0, const uint32_t* i1, float* st)
 {
-#if SW_CB_EPI == 1
-    // all-scalar form
-#pragma unroll
-    for(int t = 0; t < L; ++t) {
-        const float a = magic_f(r0[t]), b = magic_f(i0[t]), c = magic_f(r1[t]), d = magic_f(i1[t]);
-        if constexpr(STOKES <= 1) {
-            const float e0 = fadd(fmul(a, a), fmul(b, b)), e1 = fadd(fmul(c, c), fmul(d, d));
-            st[t] = STOKES == 0 ? fadd(e0, e1) : fsub(e0, e1);
-        } else if constexpr(STOKES == 2) {
-            st[t] = fmul(2.0f, fadd(fmul(a, c), fmul(b, d)));
-        } else {
-            st[t] = fmul(2.0f, fsub(fmul(b, c), fmul(a, d)));
-        }
-    }
-    return;
-#endif
+    const uint64_t Z = pack2(0.0f, 0.0f);
 #pragma unroll
     for(int t = 0; t < L; t += 2) {
         const uint64_t R0 = pair_f(r0, t), R1 = pair_f(r1, t);
         const uint64_t I0 = pair_f(i0, t), I1 = pair_f(i1, t);
-        float a0, a1, b0, b1;
-        if constexpr(SW_CB_EPI == 3) {
-            // products as fma(a, b, +0): one rounding like a multiply, and an
-            // FMA result cannot be contracted into the packed add that follows
-            const uint64_t Z = pack2(0.0f, 0.0f);
-            uint64_t S;
-            if constexpr(STOKES <= 1) {
-                const uint64_t E0 = add2(fma2(R0, R0, Z), fma2(I0, I0, Z));  // |p0|^2
-                const uint64_t E1 = add2(fma2(R1, R1, Z), fma2(I1, I1, Z));  // |p1|^2
-                S = STOKES == 0 ? add2(E0, E1) : sub2(E0, E1);
-            } else if constexpr(STOKES == 2) {
-                S = mul2(add2(fma2(R0, R1, Z), fma2(I0, I1, Z)), pack2(2.0f, 2.0f));
-            } else {
-                S = mul2(sub2(fma2(I0, R1, Z), fma2(R0, I1, Z)), pack2(2.0f, 2.0f));
-            }
-            unpack2(S, st[t], st[t + 1]);
-        } else if constexpr(STOKES <= 1 && SW_CB_EPI == 2) {
-            // packed conversion, scalar products
-            float c0, c1, d0, d1;
-            unpack2(R0, a0, a1);
-            unpack2(I0, b0, b1);
-            unpack2(R1, c0, c1);
-            unpack2(I1, d0, d1);
-            const float e00 = fadd(fmul(a0, a0), fmul(b0, b0)), e10 = fadd(fmul(c0, c0), fmul(d0, d0));
-            const float e01 = fadd(fmul(a1, a1), fmul(b1, b1)), e11 = fadd(fmul(c1, c1), fmul(d1, d1));
-            st[t]     = STOKES == 0 ? fadd(e00, e10) : fsub(e00, e10);
-            st[t + 1] = STOKES == 0 ? fadd(e01, e11) : fsub(e01, e11);
-        } else if constexpr(STOKES <= 1) {
-            float c0, c1, d0, d1;
-            unpack2(mul2(R0, R0), a0, a1);  // re0^2
-            unpack2(mul2(I0, I0), b0, b1);  // im0^2
-            unpack2(mul2(R1, R1), c0, c1);  // re1^2
-            unpack2(mul2(I1, I1), d0, d1);  // im1^2
-            const float e00 = fadd(a0, b0), e10 = fadd(c0, d0);  // |p0|^2, |p1|^2
-            const float e01 = fadd(a1, b1), e11 = fadd(c1, d1);
-            st[t]     = STOKES == 0 ? fadd(e00, e10) : fsub(e00, e10);
-            st[t + 1] = STOKES == 0 ? fadd(e01, e11) : fsub(e01, e11);
+        uint64_t S;
+        if constexpr(STOKES <= 1) {
+            const uint64_t E0 = add2(fma2(R0, R0, Z), fma2(I0, I0, Z));  // |p0|^2
+            const uint64_t E1 = add2(fma2(R1, R1, Z), fma2(I1, I1, Z));  // |p1|^2
+            S = STOKES == 0 ? add2(E0, E1) : sub2(E0, E1);
         } else if constexpr(STOKES == 2) {
             // 2*Re(p0 conj p1) = 2*(r0 r1 - i0 (-i1)) = 2*(r0 r1 + i0 i1)
-            unpack2(mul2(R0, R1), a0, a1);
-            unpack2(mul2(I0, I1), b0, b1);
-            st[t]     = fmul(2.0f, fadd(a0, b0));
-            st[t + 1] = fmul(2.0f, fadd(a1, b1));
+            S = mul2(add2(fma2(R0, R1, Z), fma2(I0, I1, Z)), pack2(2.0f, 2.0f));
         } else {
             // 2*Im(p0 conj p1) = 2*(r0 (-i1) + i0 r1) = 2*(i0 r1 - r0 i1)
-            unpack2(mul2(I0, R1), a0, a1);
-            unpack2(mul2(R0, I1), b0, b1);
-            st[t]     = fmul(2.0f, fsub(a0, b0));
-            st[t + 1] = fmul(2.0f, fsub(a1, b1));
+            S = mul2(sub2(fma2(I0, R1, Z), fma2(R0, I1, Z)), pack2(2.0f, 2.0f));
         }
+        unpack2(S, st[t], st[t + 1]);
     }
 }
 
