@@ -1,0 +1,271 @@
+// C++ stage-API tests, in the shape of the reference's gtest fixtures
+// (cpp/skyweaver/test/src/*Tester.cu), against the oracle library
+// (oracle/swb_oracle.c, the C restatement of those testers' CPU code).
+// Built and run by tests/test_gpu_cpp_api.py.  Prints "PASS <name>" per case
+// and exits non-zero on the first failure.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "skyweaver_b200.hpp"
+
+using namespace skyweaver_b200;
+
+extern "C" {
+void swo_transpose(const int8_t*, int8_t*, int, int, int, int, int, int);
+void swo_statistics(const int8_t*, float*, int, int, int, int);
+void swo_ib(const int8_t*, float*, int8_t*, int, int, int, int, const float*, const float*,
+            const float*, int, int);
+void swo_cb(const int8_t*, const int8_t*, int8_t*, int, int, int, int, int, const float*,
+            const float*, const float*, const int*, int, int, int32_t*);
+void swo_weights(const float*, int8_t*, const double*, int, int, int, double, double, double, int);
+}
+
+#define EXPECT(cond)                                                                \
+    do {                                                                            \
+        if(!(cond)) {                                                               \
+            std::fprintf(stderr, "FAILED %s:%d: %s\n", __FILE__, __LINE__, #cond);  \
+            std::exit(1);                                                           \
+        }                                                                           \
+    } while(0)
+
+static std::vector<int8_t> normal_int8(std::size_t n, float sigma, unsigned seed)
+{
+    std::mt19937 g(seed);
+    std::normal_distribution<float> d(0.0f, sigma);
+    std::vector<int8_t> v(n);
+    for(auto& x : v) x = (int8_t)std::max(-127.0f, std::min(127.0f, std::rint(d(g))));
+    return v;
+}
+
+static PipelineConfig base_config()
+{
+    PipelineConfig c;
+    c.nantennas(64);
+    c.nchans(4);
+    c.nbeams(128);
+    c.cb_tscrunch(16);
+    c.ib_tscrunch(16);
+    return c;
+}
+
+// TransposerTester.cu:119-122 parameters {12 ant, 12 heaps}, {16, 16}
+static void transposer_test()
+{
+    for(auto p : {std::pair<int, int>{12, 12}, {16, 16}}) {
+        PipelineConfig c = base_config();
+        const int A_in = p.first, H = p.second, F = (int)c.nchans(), A = (int)c.nantennas();
+        auto h = normal_int8((std::size_t)H * A_in * F * 256 * 2 * 2, 40.0f, 1);
+        DeviceBuffer<int8_t> taftp, ftpa;
+        taftp.upload(h);
+        Transposer t(c);
+        t.transpose(taftp, ftpa, A_in, nullptr);
+        std::vector<int8_t> ref((std::size_t)F * H * 256 * 2 * A * 2);
+        swo_transpose(h.data(), ref.data(), A_in, A, F, H, 256, 2);
+        EXPECT(ftpa.download() == ref);
+    }
+    std::puts("PASS transposer");
+}
+
+static void statistics_test()
+{
+    PipelineConfig c = base_config();
+    const int F = 4, A = 64, T = 1024;
+    auto h = normal_int8((std::size_t)F * T * 2 * A * 2, 20.0f, 1337);
+    DeviceBuffer<int8_t> ftpa;
+    ftpa.upload(h);
+    StatisticsCalculator s(c, nullptr);
+    s.calculate_statistics(ftpa);
+    std::vector<float> ref((std::size_t)F * 2 * A * 4);
+    swo_statistics(h.data(), ref.data(), F, T, 2, A);
+    auto got = s.statistics().download();
+    for(std::size_t i = 0; i < ref.size(); ++i)
+        EXPECT(std::fabs(got[i] - ref[i]) <= 1e-5f * std::fabs(ref[i]) + 1e-6f);
+    std::puts("PASS statistics");
+}
+
+// WeightsManagerTester.cu:99-145
+static void weights_test()
+{
+    PipelineConfig c = base_config();
+    const int A = 64, B = 128, F = 4;
+    for(int which = 0; which < 3; ++which) {
+        std::vector<float> d((std::size_t)B * A * 3);
+        for(int i = 0; i < B * A; ++i) {
+            if(which == 0) { d[3 * i] = 1.0f; d[3 * i + 1] = 0.0f; d[3 * i + 2] = 0.0f; }
+            if(which == 1) { d[3 * i] = 1.0f; d[3 * i + 1] = 1e-11f; d[3 * i + 2] = 1e-10f; }
+            if(which == 2) { d[3 * i] = i * 1e-11f; d[3 * i + 1] = i * 1e-15f; d[3 * i + 2] = 0.0f; }
+        }
+        DeviceBuffer<float> dd;
+        dd.upload(d);
+        WeightsManager wm(c, nullptr);
+        auto got = wm.weights(dd, 10.0, 9.0).download();
+        std::vector<int8_t> ref((std::size_t)F * B * A * 2);
+        swo_weights(d.data(), ref.data(), c.channel_frequencies().data(), A, B, F, 10.0, 9.0, 0.0, 1);
+        EXPECT(got == ref);
+    }
+    std::puts("PASS weights");
+}
+
+// IncoherentBeamformerTester.cu:154-210 (sigma 32, nbeamsets 1..4) and
+// CoherentBeamformerTester.cu:211-361 (weights 127 e^{i theta}, beamset_mapping[0] = 1)
+static void beamformer_tests()
+{
+    PipelineConfig c = base_config();
+    c.output_level(32.0f);
+    const int F = 4, A = 64, B = 128, T = 2048, ts = 16, S = 2;
+    auto v = normal_int8((std::size_t)F * T * 2 * A * 2, 32.0f, 7);
+    DeviceBuffer<int8_t> ftpa;
+    ftpa.upload(v);
+    const float level = 32.0f;
+    const float ib_dof = 2.0f * ts * A * 2, cb_s = std::pow(127.0f * level * std::sqrt((float)A), 2);
+    const float cb_dof = 2.0f * ts * 2;
+    std::vector<float> ib_scale(S * F, level * level * std::sqrt(2 * ib_dof) / level),
+        ib_off(S * F, level * level * ib_dof), cb_scale(S * F, cb_s * std::sqrt(2 * cb_dof) / level),
+        cb_off(S * F, cb_s * cb_dof), bw(S * A, 1.0f);
+    std::vector<int> mapping(B, 0);
+    mapping[0] = 1;
+    DeviceBuffer<float> d_ibs, d_ibo, d_cbs, d_cbo, d_bw, raw;
+    DeviceBuffer<int> d_map;
+    DeviceBuffer<int8_t> ib, cb, w;
+    d_ibs.upload(ib_scale); d_ibo.upload(ib_off); d_cbs.upload(cb_scale); d_cbo.upload(cb_off);
+    d_bw.upload(bw); d_map.upload(mapping);
+    IncoherentBeamformer ibf(c);
+    ibf.beamform(ftpa, raw, ib, d_ibs, d_ibo, d_bw, S, nullptr);
+    std::vector<float> raw_ref((std::size_t)S * (T / ts) * F);
+    std::vector<int8_t> ib_ref(raw_ref.size());
+    swo_ib(v.data(), raw_ref.data(), ib_ref.data(), F, ts, T, A, ib_scale.data(), ib_off.data(),
+           bw.data(), S, 0);
+    EXPECT(raw.download() == raw_ref);
+    EXPECT(ib.download() == ib_ref);
+    std::puts("PASS incoherent_beamformer");
+
+    std::mt19937 g(11);
+    std::uniform_real_distribution<float> u(0.0f, 6.283185307f);
+    std::vector<int8_t> hw((std::size_t)F * B * A * 2);
+    for(std::size_t i = 0; i < hw.size(); i += 2) {
+        const float th = u(g);
+        hw[i]     = (int8_t)std::lround(127.0 * std::cos(th));
+        hw[i + 1] = (int8_t)std::lround(127.0 * std::sin(th));
+    }
+    w.upload(hw);
+    CoherentBeamformer cbf(c);
+    cbf.beamform(ftpa, w, d_cbs, d_cbo, d_map, raw, cb, S, nullptr);
+    std::vector<int8_t> cb_ref((std::size_t)(T / ts) * F * B);
+    swo_cb(v.data(), hw.data(), cb_ref.data(), F, ts, T, B, A, cb_scale.data(), cb_off.data(),
+           bw.data(), mapping.data(), 0, 1, nullptr);
+    EXPECT(cb.download() == cb_ref);
+    std::puts("PASS coherent_beamformer");
+}
+
+// IncoherentDedisperserTester.cu:39-126
+static void incoherent_dedisperser_tests()
+{
+    PipelineConfig c = base_config();
+    c.nchans(64);
+    c.nbeams(32);
+    {
+        IncoherentDedisperser d(c, 0.0f);
+        for(int x : d.delays()) EXPECT(x == 0);
+        EXPECT(d.max_sample_delay() == 0);
+    }
+    c.bandwidth(32e6);
+    c.centre_frequency(580e6);
+    std::vector<float> dms = {0.0f, 10.0f, 20.0f, 30.0f, 40.0f};
+    for(std::size_t ts : {1, 2}) {
+        IncoherentDedisperser d(c, dms, ts);
+        EXPECT(d.max_sample_delay() > 0);
+        std::size_t T = 3 * d.max_sample_delay();
+        T -= (T - d.max_sample_delay()) % ts;
+        DeviceBuffer<int8_t> tfb, tdb;
+        tfb.upload(std::vector<int8_t>(T * c.nchans() * c.nbeams(), 1));
+        d.dedisperse(tfb, tdb);
+        const auto out = tdb.download();
+        EXPECT(out.size() == (T - d.max_sample_delay()) / ts * dms.size() * c.nbeams());
+        for(int8_t x : out) EXPECT(x == (int8_t)std::sqrt((double)(c.nchans() * ts)));
+    }
+    {
+        IncoherentDedisperser d(c, dms);
+        DeviceBuffer<int8_t> tfb, tdb;
+        tfb.upload(std::vector<int8_t>(d.max_sample_delay() * c.nchans() * c.nbeams(), 0));
+        bool threw = false;
+        try { d.dedisperse(tfb, tdb); } catch(const std::runtime_error&) { threw = true; }
+        EXPECT(threw);
+    }
+    std::puts("PASS incoherent_dedisperser");
+}
+
+// DelayManagerTester.cu:38-52 with the reference's test_delays.bin
+static void delay_manager_tests(const std::string& golden)
+{
+    PipelineConfig c = base_config();
+    c.delay_file(golden + "/test_delays.bin");
+    DelayManager dm(c, nullptr);
+    EXPECT(dm.nbeamsets() == 2);
+    EXPECT(dm.beamset_weights().size() == 2 * c.nantennas());
+    EXPECT(std::fabs(dm.epoch() - 1708082168.957) < 1e-3);
+    const auto& d = dm.delays(dm.epoch() + 1.0);
+    EXPECT(d.size() == c.nbeams() * c.nantennas() * 3);
+    bool threw = false;
+    try { dm.delays(dm.epoch() - 10.0); } catch(const InvalidDelayEpoch&) { threw = true; }
+    EXPECT(threw);
+    threw = false;
+    try { dm.delays(1e10); } catch(const std::runtime_error&) { threw = true; }
+    EXPECT(threw);
+    std::puts("PASS delay_manager");
+}
+
+static void dedispersion_plan_tests()
+{
+    DedispersionPlan p;
+    p.add_block("10.0");
+    p.add_block("20.0:4");
+    p.add_block("30.0:25.0:35.0:2.0:8");
+    EXPECT(p.coherent_dms().size() == 3);
+    EXPECT(p[1].tscrunch == 4);
+    EXPECT(p[2].incoherent_dms.size() == 5);
+    bool threw = false;
+    try { p.add_block("1:2:3"); } catch(const std::runtime_error&) { threw = true; }
+    EXPECT(threw);
+    std::puts("PASS dedispersion_plan");
+}
+
+struct CountingHandler {
+    std::size_t calls = 0, bytes = 0;
+    void operator()(const int8_t*, std::size_t n, std::size_t) { ++calls; bytes += n; }
+};
+
+// BeamformerPipelineTester.cu:119-167 (zeros through the full chain)
+static void pipeline_smoke(const std::string& golden)
+{
+    PipelineConfig c = base_config();
+    c.delay_file(golden + "/test_delays.bin");
+    c.gulp_length_samps(4096);
+    c.ddplan().add_block(0.0f);
+    c.ddplan().add_block(5.0f);
+    CountingHandler h;
+    BeamformerPipeline<CountingHandler> pipe(c, h, 57);
+    std::vector<int8_t> taftp((std::size_t)16 * 57 * c.nchans() * 256 * 2 * 2, 0);
+    for(int g = 0; g < 3; ++g) pipe(taftp.data(), 1708082168.957 + 1.0 + g * 0.02);
+    EXPECT(h.calls == 6);
+    EXPECT(h.bytes == 6 * (4096 / 16) * c.nchans() * c.nbeams());
+    std::puts("PASS beamformer_pipeline");
+}
+
+int main(int argc, char** argv)
+{
+    const std::string golden = argc > 1 ? argv[1] : "tests/golden";
+    transposer_test();
+    statistics_test();
+    weights_test();
+    beamformer_tests();
+    incoherent_dedisperser_tests();
+    delay_manager_tests(golden);
+    dedispersion_plan_tests();
+    pipeline_smoke(golden);
+    std::puts("ALL PASS");
+    return 0;
+}
