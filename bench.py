@@ -36,6 +36,9 @@ sys.path.insert(0, REPO)
 WORK = dict(nant=64, nbeams=1024, nchans=64, gulp=65536, tscrunch=16,
             dms=[0.0, 50.0, 150.0, 500.0], centre=1284e6, chbw=856e6 / 1024)
 METRIC = "real-time factor & int8 TOPS, 64ant×1024beam×4DM: batched vs plain GPU"
+# dram__bytes_read.sum + dram__bytes_write.sum of one cb_kernel<16,0> launch on
+# the 16-channel, one-DM case of `bench.py --profile cb` (ncu --set full).
+CB_NCU_BYTES_16CH_1DM = 273.018368e6 + 55.531008e6
 
 
 def tsamp():
@@ -177,6 +180,28 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+# ------------------------------------------------------- rank decomposition
+def rank_subband(rank, world):
+    """Centre frequency and bandwidth of the subband that `rank` of `world`
+    beamforms: adjacent, non-overlapping blocks of WORK["nchans"] channels
+    centred on the band centre (weak scaling; subbands share no data, so
+    no collective sits on the data path)."""
+    bw = WORK["nchans"] * WORK["chbw"]
+    return WORK["centre"] + (rank - (world - 1) / 2) * bw, bw
+
+
+def max_over_ranks(value, world, device=None):
+    """Max of a per-rank device time over the process group (the job takes
+    as long as its slowest rank)."""
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 # ---------------------------------------------------------------- B200 arm
 def main_b200(args):
     import torch
@@ -196,9 +221,7 @@ def main_b200(args):
 
     A, B, F, T, ts = WORK["nant"], WORK["nbeams"], WORK["nchans"], WORK["gulp"], WORK["tscrunch"]
     dms = WORK["dms"]
-    # each rank beamforms its own 64-channel subband (weak scaling, no exchange)
-    centre = WORK["centre"] + (rank - (world - 1) / 2) * F * WORK["chbw"]
-    bwidth = F * WORK["chbw"]
+    centre, bwidth = rank_subband(rank, world)
     g = synthetic.rng(1000 + rank)
     delays = synthetic.delay_model(g, B, A)
     gen = torch.Generator(device="cuda").manual_seed(1234 + rank)
@@ -232,12 +255,7 @@ def main_b200(args):
             fn(W + i)
         e1.record(stream)
         barrier()
-        ms = e0.elapsed_time(e1)
-        if world > 1:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms / K
+        return max_over_ranks(e0.elapsed_time(e1), world, "cuda") / K
 
     # ---- headline: batched grouped CB + CUDA graph, input resident in HBM
     with Clocks(local) as clk:
@@ -278,9 +296,16 @@ def main_b200(args):
     int8_peak = 2.0 * peaks.get("bf16_tflops", 1590.0)      # dense int8 = 2x dense bf16
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
     cb = kern["coherent_beamformer"]
+    # DRAM bytes of one cb_kernel launch from the ncu capture of the 16-channel,
+    # one-DM profile case (dram__bytes_read.sum 273.0 MB + write 55.5 MB),
+    # scaled by the channels x DMs one grouped launch processes.
+    traffic = CB_NCU_BYTES_16CH_1DM * (F / 16.0) * len(dms)
+    algo_bytes = len(dms) * (F * 2 * A * 2 * T + (T // WORK["tscrunch"]) * F * B)
     roof = {"bound": "tensor", "kernel": "coherent_beamformer (tcgen05 kind::i8, grouped)",
             "achieved": cb["tops"], "peak": int8_peak, "unit": "TOPS (int8)",
-            "frac": cb["tops"] / int8_peak, "traffic": None,
+            "frac": cb["tops"] / int8_peak, "traffic": traffic,
+            "traffic_unit": "DRAM bytes per launch (ncu, 16-channel case scaled)",
+            "algorithmic_bytes": algo_bytes,
             "peak_source": "2x measured bf16 cuBLAS burst (MEASURED_PEAKS.json)"
             if peaks else "2x fallback bf16 1.59 PFLOP/s"}
     ops_gulp = 8.0 * A * B * 2 * F * T * len(dms)
