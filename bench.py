@@ -277,6 +277,9 @@ def main_b200(args):
     kern = kernel_breakdown(torch, stages, taftp, delays, fft_len, overlap, centre, bwidth,
                             args.steps)
 
+    # ---- ragged (DM x beamset) problems: grouped vs plain
+    ragged = ragged_case(torch, stages, synthetic, args.steps)
+
     # ---- end to end through the host API (pinned H2D + D2H inside the timing)
     h_in = torch.empty(taftp.shape, dtype=torch.int8, pin_memory=True)
     h_in.copy_(taftp)
@@ -319,7 +322,7 @@ def main_b200(args):
             "int8_tops_pipeline": ops_gulp / (ms_graph * 1e-3) / 1e12,
             "cb_int8_tops": cb["tops"],
             "plain": {"value": gulp_s / (ms_plain * 1e-3) * world, "ms_per_step": ms_plain},
-            "batched_vs_plain": ms_plain / ms_graph,
+            "batched_vs_plain": ms_plain / ms_graph, "ragged": ragged,
             "kernels": kern, "roofline": roof, "hbm_peak_gbs": hbm_peak, "e2e": e2e,
             "gpu_launches": launches * args.steps, "clocks": clocks}
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -391,6 +394,90 @@ def kernel_breakdown(torch, stages, taftp, delays, fft_len, overlap, centre, bwi
         if k != "coherent_beamformer_plain":
             v["share"] = v["ms"] / total
     return out
+
+
+RAGGED = dict(nant=64, nchans=64, gulp=32768, tscrunch=16, dms=[0.0, 50.0, 150.0, 500.0],
+              ants=[64, 57, 48, 40, 32, 24, 16, 8], beams=[512, 256, 256, 128, 128, 64, 64, 32])
+
+
+def ragged_case(torch, stages, synthetic, K):
+    """Ragged batched beamforming: 8 beamsets with antenna masks of
+    {64..8} antennas and {512..32} beams, x 4 coherent DMs = 32 (DM, beamset)
+    GEMM problems, 64 channels, 32768-sample gulps.  The grouped form is one
+    persistent launch over all of them (128-beam tiles pack across beamset
+    boundaries); the plain form is one launch per (DM, beamset).  Credited
+    int8 ops count active antennas only: 8 * sum(A_s * B_s) * P * F * T per DM.
+    Also times the whole pipeline both ways (graph + grouped vs eager + plain)."""
+    R = RAGGED
+    A, F, T, ts, dms = R["nant"], R["nchans"], R["gulp"], R["tscrunch"], R["dms"]
+    B = sum(R["beams"])
+    g = synthetic.rng(31)
+    masks = synthetic.beamset_masks(g, A, R["ants"])
+    mapping = np.repeat(np.arange(len(R["beams"]), dtype=np.int32), R["beams"])
+    delays = synthetic.delay_model(g, B, A)
+    delays[..., 0] = masks[mapping]
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    stream = torch.cuda.current_stream()
+
+    def timeit(fn, reps=K, warm=3):
+        for _ in range(warm):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    gen = torch.Generator(device="cuda").manual_seed(99)
+    fps = [(torch.randn((F, 2, A, 2, T), generator=gen, device="cuda") * 8).round_()
+           .clamp_(-127, 127).to(torch.int8) for _ in dms]
+    freqs = stages.channel_frequencies(WORK["centre"], F * WORK["chbw"], F)
+    _, gemm = stages.generate_weights(dev(delays), dev(freqs), 0.0, 0.0, want_fba=False)
+    S = len(R["beams"])
+    scl = dev(np.full(S * F, 1e9, np.float32))
+    d_map = dev(mapping)
+    raws = [torch.rand((S, T // ts, F), device="cuda") for _ in dms]
+    outs = [torch.empty((T // ts, F, B), dtype=torch.int8, device="cuda") for _ in dms]
+    starts = np.concatenate([[0], np.cumsum(R["beams"])[:-1]])
+    grouped = [(fp, o, r, 0, B) for fp, o, r in zip(fps, outs, raws)]
+    plain = [(fp, o, r, int(b0), int(nb)) for fp, o, r in zip(fps, outs, raws)
+             for b0, nb in zip(starts, R["beams"])]
+    ms_g = timeit(lambda: stages.coherent_beamform_grouped(grouped, gemm, scl, scl, d_map, T, ts))
+    ref = [o.clone() for o in outs]
+    ms_p = timeit(lambda: [stages.coherent_beamform(p[0], gemm, scl, scl, d_map, p[2], T, ts,
+                                                    beam_start=p[3], beam_count=p[4], out=p[1])
+                           for p in plain])
+    same = all(torch.equal(a, b) for a, b in zip(ref, outs))
+    credited = 8.0 * float(np.dot(R["ants"], R["beams"])) * 2 * F * T * len(dms)
+    del fps, outs, raws
+    # whole pipeline, both forms
+    bw = F * WORK["chbw"]
+    common = dict(nantennas=A, input_nantennas=A, nchans=F, nbeams=B, gulp_samples=T,
+                  tscrunch=ts, centre_frequency=WORK["centre"], bandwidth=bw, dms=dms,
+                  beamset_weights=masks, beamset_mapping=mapping)
+    taftp = (torch.randn((T // 256, A, F, 256, 2, 2), generator=gen, device="cuda") * 8.0)
+    taftp = taftp.round_().clamp_(-127, 127).to(torch.int8)
+    gulp_s = T / WORK["chbw"]
+    res = {}
+    for name, kw in (("grouped_graph", dict(grouped=True, use_graph=True)),
+                     ("plain_eager", dict(grouped=False, use_graph=False))):
+        p = stages.BeamformerPipeline(**common, **kw)
+        p.set_delays(delays, 1.7e9)
+        res[name] = timeit(lambda: p.process_device(taftp, 1.7e9), reps=max(3, K // 2))
+        p.close()
+    return {"workload": "8 beamsets, antennas {64,57,48,40,32,24,16,8}, beams "
+                        "{512,256,256,128,128,64,64,32}, x4 DMs = 32 problems, 64 ch, "
+                        "32768-sample gulps",
+            "cb_grouped_ms": ms_g, "cb_plain_ms": ms_p, "cb_grouped_vs_plain": ms_p / ms_g,
+            "cb_grouped_tops_credited": credited / (ms_g * 1e-3) / 1e12,
+            "cb_plain_tops_credited": credited / (ms_p * 1e-3) / 1e12,
+            "cb_outputs_identical": bool(same),
+            "pipeline_grouped_graph_rtf": gulp_s / (res["grouped_graph"] * 1e-3),
+            "pipeline_plain_eager_rtf": gulp_s / (res["plain_eager"] * 1e-3),
+            "pipeline_grouped_vs_plain": res["plain_eager"] / res["grouped_graph"]}
 
 
 def profile_case(which, nchans=16, reps=3):

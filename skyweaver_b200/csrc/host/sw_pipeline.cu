@@ -260,28 +260,36 @@ int sw_pipeline::enqueue_chain(const void* d_in, int parity, bool first)
                                       ib_i8[parity][d].as<int8_t>(), ss));
     }
     sw_cb_shape shape{F, T, A, B, ts, cfg.stokes, cfg.ib_subtract, vstride, voff};
-    // problems: one per (DM, contiguous run of beams in the same beamset)
-    std::vector<sw_cb_problem> probs;
-    for(int d = 0; d < ndm; ++d) {
-        int b = 0;
-        while(b < B) {
-            int e = b + 1;
-            while(e < B && mapping[e] == mapping[b]) ++e;
-            probs.push_back({volt[d], cb[parity][d].as<int8_t>(), ib_raw[parity][d].as<float>(),
-                             b, e - b});
-            b = e;
-        }
-    }
-    if(probs.size() > 96) {  // too ragged for one launch table: one range per DM
-        probs.clear();
+    if(cfg.grouped) {
+        // one problem per DM over all beams: the epilogue resolves each beam's
+        // beamset (scale, offset, IB power) itself, so 128-beam tiles pack
+        // across beamset boundaries and every (DM, beamset) shares one queue
+        std::vector<sw_cb_problem> probs;
         for(int d = 0; d < ndm; ++d)
             probs.push_back({volt[d], cb[parity][d].as<int8_t>(), ib_raw[parity][d].as<float>(), 0, B});
-    }
-    if(cfg.grouped) {
         SW_TRY(sw_coherent_beamform_grouped(&shape, probs.data(), (int)probs.size(), d_wgemm.p,
                                             cb_scl.as<float>(), cb_off.as<float>(),
                                             d_map.as<int>(), ss));
     } else {
+        // plain form: one launch per (DM, contiguous run of beams of one
+        // beamset); a mapping with more than 96 runs falls back to one launch
+        // per DM
+        std::vector<sw_cb_problem> probs;
+        for(int d = 0; d < ndm; ++d) {
+            int b = 0;
+            while(b < B) {
+                int e = b + 1;
+                while(e < B && mapping[e] == mapping[b]) ++e;
+                probs.push_back({volt[d], cb[parity][d].as<int8_t>(),
+                                 ib_raw[parity][d].as<float>(), b, e - b});
+                b = e;
+            }
+        }
+        if(probs.size() > 96) {
+            probs.clear();
+            for(int d = 0; d < ndm; ++d)
+                probs.push_back({volt[d], cb[parity][d].as<int8_t>(), ib_raw[parity][d].as<float>(), 0, B});
+        }
         for(auto& pr : probs)
             SW_TRY(sw_coherent_beamform(&shape, &pr, d_wgemm.p, cb_scl.as<float>(),
                                         cb_off.as<float>(), d_map.as<int>(), nullptr, ss));

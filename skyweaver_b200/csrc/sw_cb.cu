@@ -263,17 +263,14 @@ __device__ __forceinline__ uint64_t sub2(uint64_t a, uint64_t b)
     return d;
 }
 
-// Exact int32 -> float without the low-throughput I2F conversion: every
-// accumulator element starts at the bit pattern of 1.5*2^23 (0x4B400000)
-// and the MMAs add the int32 sum v to it.  For |v| < 2^22 (beam voltages
-// stay below 2^21 for up to 64 antennas) the result is the float
-// 1.5*2^23 + v exactly, and subtracting 1.5*2^23 in float recovers v.
-constexpr uint32_t kMagicBits = 0x4B400000u;  // 12582912.0f
-
+// Exact int32 -> float: every beam voltage is below 2^21 in magnitude, so the
+// round-to-nearest conversion is exact.  (Measured against a magic-constant
+// scheme, 1.5*2^23 preloaded into TMEM and subtracted in float, and against
+// an integer add of that constant: the plain conversion was fastest, since
+// it needs no TMEM re-arm and no constant registers.)
 __device__ __forceinline__ uint64_t pair_f(const uint32_t* w, int t)
 {
-    return sub2(pack2(__uint_as_float(w[t]), __uint_as_float(w[t + 1])),
-                pack2(12582912.0f, 12582912.0f));
+    return pack2(__int2float_rn((int)w[t]), __int2float_rn((int)w[t + 1]));
 }
 
 // Stokes of L consecutive samples from the exact beam voltages
@@ -415,8 +412,8 @@ cb_kernel(const __grid_constant__ Params P)
                 bool ok = true;
                 for(int tile = tile0; tile < tile1; ++tile) {
                     if(!mbar_wait(&v_full[vs], vph, s_abort, deadline, P.err)) { ok = false; break; }
-                    // phase 0 of acc_empty is completed by the epilogue's
-                    // initial fill of both buffers with the magic constant
+                    // phase 0 of acc_empty is completed by the epilogue
+                    // warps' initial arrival (both buffers start free)
                     if(!mbar_wait(&acc_empty[ab], aph, s_abort, deadline, P.err)) { ok = false; break; }
                     fence_after();
                     const uint32_t vb = smem_u32(vbuf + vs * vtile);
@@ -426,10 +423,9 @@ cb_kernel(const __grid_constant__ Params P)
                         const uint64_t adr = make_desc(wa + ks * 32, 1, P.w_sbo16, P.w_layout);
                         const uint64_t adi = make_desc(wa + wtile + ks * 32, 1, P.w_sbo16, P.w_layout);
                         const uint64_t bd  = make_desc(vb + ks * 2048, P.v_lbo16, 32, 4 /*SW64*/);
-                        // always accumulate: the buffer holds 0x4B400000
-                        // per element, so D = 1.5*2^23 (as float bits) + sum
-                        mma_i8(d_re, adr, bd, P.idesc, 1);
-                        mma_i8(d_im, adi, bd, P.idesc, 1);
+                        // the first K step overwrites the buffer
+                        mma_i8(d_re, adr, bd, P.idesc, ks > 0);
+                        mma_i8(d_im, adi, bd, P.idesc, ks > 0);
                     }
                     mma_commit(&v_empty[vs]);
                     mma_commit(&acc_full[ab]);
@@ -450,19 +446,7 @@ cb_kernel(const __grid_constant__ Params P)
         const int F = P.nchans;
         const int nout = P.nsamples / TS;
         const uint32_t lane_base = tmem + ((uint32_t)(q * 32) << 16);
-        uint32_t magic[8];
-#pragma unroll
-        for(int k = 0; k < 8; ++k) magic[k] = kMagicBits;
-        // fill this warp's columns of both accumulator buffers with the magic
-        // constant, then release both buffers to the MMA warp (phase 0)
-#pragma unroll
-        for(int buf = 0; buf < 2; ++buf)
-#pragma unroll
-            for(int g = 0; g < kGroups; ++g)
-#pragma unroll
-                for(int sec = 0; sec < 4; ++sec)
-                    SW_TMEM_ST8(lane_base + buf * 256 + sec * 64 + h * kSlice + g * 8, magic);
-        tmem_wait_st();
+        // release both accumulator buffers to the MMA warp (phase 0)
         fence_before();
         __syncwarp();
         if(lane == 0) { mbar_arrive(&acc_empty[0]); mbar_arrive(&acc_empty[1]); }
@@ -492,20 +476,15 @@ cb_kernel(const __grid_constant__ Params P)
                     SW_TMEM_LD8(ta + 128, i0);
                     SW_TMEM_LD8(ta + 192, i1);
                     tmem_wait_ld();
-                    // re-arm these columns for the next tile that uses this buffer
-                    SW_TMEM_ST8(ta, magic);
-                    SW_TMEM_ST8(ta + 64, magic);
-                    SW_TMEM_ST8(ta + 128, magic);
-                    SW_TMEM_ST8(ta + 192, magic);
                     const int tbase = tile * kTileT + h * kSlice + g * 8;
                     if(P.debug != nullptr && valid) {
                         int2* dbg = reinterpret_cast<int2*>(P.debug);
                         for(int t = 0; t < 8; ++t) {
                             const size_t base_t = (size_t)it.f * P.nsamples + tbase + t;
                             dbg[(base_t * 2 + 0) * P.nbeams + b] =
-                                make_int2((int)(r0[t] - kMagicBits), (int)(i0[t] - kMagicBits));
+                                make_int2((int)r0[t], (int)i0[t]);
                             dbg[(base_t * 2 + 1) * P.nbeams + b] =
-                                make_int2((int)(r1[t] - kMagicBits), (int)(i1[t] - kMagicBits));
+                                make_int2((int)r1[t], (int)i1[t]);
                         }
                     }
                     float st[8];
@@ -531,7 +510,6 @@ cb_kernel(const __grid_constant__ Params P)
                         }
                     }
                 }
-                tmem_wait_st();
                 fence_before();
                 __syncwarp();
                 if(lane == 0) mbar_arrive(&acc_empty[ab]);

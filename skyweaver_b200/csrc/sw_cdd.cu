@@ -211,7 +211,7 @@ struct Args {
     int nseg;
     int ndms;
     const c32* tw;     // twiddle tables
-    const c32* chirp;  // [ndms][F][N] digit-reversed
+    const c32* chirp;  // [ndms][F][N] in per-thread load order (chirp_k)
     int npa;           // P * A (streams per channel)
     uint8_t* out[kMaxDms];
     size_t out_stride;
@@ -409,10 +409,10 @@ cdd_kernel(const __grid_constant__ Args A)
         dft16<false>(spec);
 
         const size_t chirp_stride = (size_t)(A.nstreams / A.npa) * N;  // per DM
-        const float4* chp = reinterpret_cast<const float4*>(A.chirp + (size_t)f * N + threadIdx.x * 16);
+        const float4* chp = reinterpret_cast<const float4*>(A.chirp + (size_t)f * N) + threadIdx.x;
         float4 chn[8];
 #pragma unroll
-        for(int k = 0; k < 8; ++k) chn[k] = chp[k];
+        for(int k = 0; k < 8; ++k) chn[k] = chp[k * NT];
         __syncthreads();
 
         for(int d = 0; d < A.ndms; ++d) {
@@ -425,7 +425,7 @@ cdd_kernel(const __grid_constant__ Args A)
             if(d + 1 < A.ndms) {  // next DM's chirp, in flight during this inverse
                 const float4* nxt = chp + (size_t)(d + 1) * chirp_stride / 2;
 #pragma unroll
-                for(int k = 0; k < 8; ++k) chn[k] = nxt[k];
+                for(int k = 0; k < 8; ++k) chn[k] = nxt[k * NT];
             }
             dft16<true>(y);
 #pragma unroll
@@ -504,18 +504,24 @@ __global__ void twiddle_k(c32* tw, int logn)
     }
 }
 
-// DMResponse (CoherentDedisperser.cu:313-335) in FP64, stored at the
-// digit-reversed position of its bin.
+// DMResponse (CoherentDedisperser.cu:313-335) in FP64.  The transform
+// leaves bin digit_reverse(16 t + r) in register r of thread t; the table
+// stores the chirp of that bin at ((r / 2) * (N / 16) + t) * 2 + r % 2, so
+// that the k-th 16-byte load of every thread (registers 2k and 2k+1) reads
+// one contiguous 512-byte span per warp.
 __global__ void chirp_k(c32* chirp, SetupArgs S)
 {
     const Plan P = make_plan(S.logn);
+    const int nt = P.n / 16;
     const size_t total = (size_t)S.ndms * S.nchans * P.n;
     for(size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total;
         i += (size_t)gridDim.x * blockDim.x) {
-        const int pos = (int)(i % P.n);
+        const int q   = (int)(i % P.n);
         const int c   = (int)((i / P.n) % S.nchans);
         const int d   = (int)(i / ((size_t)P.n * S.nchans));
-        const int k   = digit_reverse(P, pos);
+        const int t   = (q >> 1) % nt;
+        const int r   = 2 * ((q >> 1) / nt) + (q & 1);
+        const int k   = digit_reverse(P, 16 * t + r);
         const double nu0   = S.low_freq + c * S.coarse_bw - 0.5 * S.coarse_bw;
         const double nu    = k * S.fine_bw;
         const double phase = (nu * nu * S.prefactor[d]) / ((nu0 + nu) * nu0 * nu0);
