@@ -52,7 +52,11 @@ enum sw_status {
     SW_ERR_EPOCH       = 6  /* InvalidDelayEpoch (DelayManager.cuh:19-34) */
 };
 
-enum sw_stokes { SW_STOKES_I = 0, SW_STOKES_Q = 1, SW_STOKES_U = 2, SW_STOKES_V = 3 };
+/* Stokes modes: one parameter (int8 outputs, float raw IB power) or all four
+ * (SW_STOKES_IQUV: char4 {I,Q,U,V} outputs and float4 raw IB power, the
+ * reference's FullStokesBeamformerTraits, beamformer_utils.cuh:198-278). */
+enum sw_stokes { SW_STOKES_I = 0, SW_STOKES_Q = 1, SW_STOKES_U = 2, SW_STOKES_V = 3,
+                 SW_STOKES_IQUV = 4 };
 
 /* Library identification and error reporting. */
 int sw_version(void);

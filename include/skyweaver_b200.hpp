@@ -179,13 +179,17 @@ class PipelineConfig {
         }
         return _freqs;
     }
+    // "I", "Q", "U", "V" (SingleStokesBeamformerTraits) or "IQUV"
+    // (FullStokesBeamformerTraits: char4 / float4 outputs)
     int stokes_index() const
     {
-        static const char* names[] = {"I", "Q", "U", "V"};
-        for(int i = 0; i < 4; ++i)
+        static const char* names[] = {"I", "Q", "U", "V", "IQUV"};
+        for(int i = 0; i < 5; ++i)
             if(_stokes == names[i]) return i;
         throw std::runtime_error("Unsupported Stokes mode: " + _stokes);
     }
+    // values per output sample: 4 for IQUV, else 1
+    std::size_t stokes_components() const { return stokes_index() == 4 ? 4 : 1; }
 
   private:
     std::size_t _nant = 64, _nchans = 64, _nbeams = 32, _cb_ts = 16, _ib_ts = 16, _gulp = 4096;
@@ -435,8 +439,8 @@ class IncoherentBeamformer {
         const std::size_t F = _config.nchans(), A = _config.nantennas(), ts = _config.ib_tscrunch();
         const std::size_t T = ftpa.size() / (F * 2 * A * 2);
         ftpa_to_fpact(ftpa, _fpact, F, T, A, stream);
-        output_raw.resize(nbeamsets * (T / ts) * F);
-        output.resize(nbeamsets * (T / ts) * F);
+        output_raw.resize(nbeamsets * (T / ts) * F * _config.stokes_components());
+        output.resize(nbeamsets * (T / ts) * F * _config.stokes_components());
         check(sw_incoherent_beamform(_fpact.data(), T, 0, (int)F, (int)T, (int)A, (int)ts,
                                      output_scale.data(), output_offset.data(),
                                      antenna_weights.data(), nbeamsets, _config.stokes_index(),
@@ -472,7 +476,7 @@ class CoherentBeamformer {
         ftpa_to_fpact(ftpa, _fpact, F, T, A, stream);
         _gemm.resize(2 * weights.size());
         check(sw_pack_weights(weights.data(), _gemm.data(), (int)F, (int)B, (int)A, (sw_stream_t)stream));
-        output.resize((T / ts) * F * B);
+        output.resize((T / ts) * F * B * _config.stokes_components());
         sw_cb_shape shape{(int)F, (int)T, (int)A, (int)B, (int)ts, _config.stokes_index(),
                           _config.ib_subtraction() ? 1 : 0, T, 0};
         sw_cb_problem prob{_fpact.data(), output.data(), ib_powers.data(), 0, (int)B};
@@ -519,7 +523,22 @@ class IncoherentDedisperser {
     // int8 TFB [T][F][B] -> int8 TDB [(T - max_delay)/tscrunch][ndms][B]
     void dedisperse(const DeviceBuffer<int8_t>& tfb, DeviceBuffer<int8_t>& tdb, cudaStream_t stream = 0)
     {
-        const std::size_t F = _config.nchans(), B = _config.nbeams();
+        run(tfb, tdb, 1, stream);
+    }
+    // char4 (IQUV) TFB -> char4 TDB, each component dedispersed and clamped
+    // independently like the reference's char4 instantiation
+    // (IncoherentDedisperser.cu:133-137); buffers hold 4 int8 per sample
+    void dedisperse_iquv(const DeviceBuffer<int8_t>& tfb, DeviceBuffer<int8_t>& tdb,
+                         cudaStream_t stream = 0)
+    {
+        run(tfb, tdb, 4, stream);
+    }
+
+  private:
+    void run(const DeviceBuffer<int8_t>& tfb, DeviceBuffer<int8_t>& tdb, std::size_t ncomp,
+             cudaStream_t stream)
+    {
+        const std::size_t F = _config.nchans(), B = _config.nbeams() * ncomp;
         const std::size_t T = tfb.size() / (F * B);
         if(T <= (std::size_t)_max)
             throw std::runtime_error("Fewer than max_sample_delay samples passed to dedisperse method");
@@ -532,7 +551,6 @@ class IncoherentDedisperser {
         cuda_check(cudaStreamSynchronize(stream), "incoherent dedispersion");
     }
 
-  private:
     const PipelineConfig& _config;
     std::vector<float> _dms;
     std::size_t _tscrunch;

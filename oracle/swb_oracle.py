@@ -96,7 +96,17 @@ def scalings(stats, beamset_weights, nbeamsets, cb_tscrunch, ib_tscrunch,
 # ---------------------------------------------------------------- IB and CB
 def incoherent_beam(ftpa, tscrunch, scale, offset, beamset_weights, nbeamsets,
                     stokes="I"):
-    """IncoherentBeamformerTester.cu:41-103 -> (raw float BTF, int8 BTF)."""
+    """IncoherentBeamformerTester.cu:41-103 -> (raw float BTF, int8 BTF).
+
+    stokes="IQUV" follows FullStokesBeamformerTraits (beamformer_utils.cuh:
+    198-278): every member (integrate, ib_subtract, rescale, clamp) applies
+    the single-Stokes trait of its component, so component c of the float4 /
+    char4 result is the single-Stokes result for c; the arrays gain a last
+    axis of 4."""
+    if stokes == "IQUV":
+        parts = [incoherent_beam(ftpa, tscrunch, scale, offset, beamset_weights, nbeamsets, c)
+                 for c in "IQUV"]
+        return (np.stack([p[0] for p in parts], -1), np.stack([p[1] for p in parts], -1))
     ftpa = _c(ftpa, np.int8)
     nchans, nsamp, npol, nant, _ = ftpa.shape
     raw = np.empty((nbeamsets, nsamp // tscrunch, nchans), np.float32)
@@ -110,7 +120,15 @@ def incoherent_beam(ftpa, tscrunch, scale, offset, beamset_weights, nbeamsets,
 def coherent_beam(ftpa, weights, tscrunch, scales, offsets, beamset_weights,
                   mapping, stokes="I", ib_subtract=True, want_voltages=False):
     """CoherentBeamformerTester.cu:43-152 -> int8 TFB [T/ts][F][B]
-    (and optionally the exact int32 beam voltages [F][T][P][B][2])."""
+    (and optionally the exact int32 beam voltages [F][T][P][B][2]).
+    stokes="IQUV": char4 TFB [T/ts][F][B][4], component c equal to the
+    single-Stokes result for c (FullStokesBeamformerTraits)."""
+    if stokes == "IQUV":
+        parts = [coherent_beam(ftpa, weights, tscrunch, scales, offsets, beamset_weights,
+                               mapping, c, ib_subtract, want_voltages) for c in "IQUV"]
+        if want_voltages:
+            return np.stack([p[0] for p in parts], -1), parts[0][1]
+        return np.stack(parts, -1)
     ftpa = _c(ftpa, np.int8)
     weights = _c(weights, np.int8)
     nchans, nsamp, npol, nant, _ = ftpa.shape

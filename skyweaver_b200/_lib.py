@@ -16,7 +16,7 @@ c_void_p = ctypes.c_void_p
 c_float_p = ctypes.POINTER(ctypes.c_float)
 
 SW_OK = 0
-STOKES = {"I": 0, "Q": 1, "U": 2, "V": 3}
+STOKES = {"I": 0, "Q": 1, "U": 2, "V": 3, "IQUV": 4}
 
 
 class SkyweaverError(RuntimeError):

@@ -104,8 +104,10 @@ struct sw_pipeline {
         if(h_epochs) cudaFreeHost(h_epochs);
     }
 
-    size_t cb_bytes() const { return (size_t)(T / ts) * F * B; }
-    size_t ib_elems() const { return (size_t)S * (T / ts) * F; }
+    // IQUV (stokes 4) carries four components per sample: char4 / float4
+    int ncomp() const { return cfg.stokes == 4 ? 4 : 1; }
+    size_t cb_bytes() const { return (size_t)(T / ts) * F * B * ncomp(); }
+    size_t ib_elems() const { return (size_t)S * (T / ts) * F * ncomp(); }
 
     int init(const sw_pipeline_config& c);
     int enqueue_chain(const void* d_in, int parity, bool first);

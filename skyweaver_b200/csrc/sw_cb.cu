@@ -306,6 +306,28 @@ __device__ __forceinline__ void stokes_n(const uint32_t* r0, const uint32_t* r1,
     }
 }
 
+// All four Stokes parameters (FullStokesBeamformerTraits,
+// beamformer_utils.cuh:198-278): component c is computed exactly like the
+// single-Stokes mode c, so st[c] equals stokes_n<c> element for element.
+template <int L>
+__device__ __forceinline__ void stokes_iquv(const uint32_t* r0, const uint32_t* r1,
+                                            const uint32_t* i0, const uint32_t* i1,
+                                            float (*st)[L])
+{
+    const uint64_t Z = pack2(0.0f, 0.0f), two = pack2(2.0f, 2.0f);
+#pragma unroll
+    for(int t = 0; t < L; t += 2) {
+        const uint64_t R0 = pair_f(r0, t), R1 = pair_f(r1, t);
+        const uint64_t I0 = pair_f(i0, t), I1 = pair_f(i1, t);
+        const uint64_t E0 = add2(fma2(R0, R0, Z), fma2(I0, I0, Z));
+        const uint64_t E1 = add2(fma2(R1, R1, Z), fma2(I1, I1, Z));
+        unpack2(add2(E0, E1), st[0][t], st[0][t + 1]);
+        unpack2(sub2(E0, E1), st[1][t], st[1][t + 1]);
+        unpack2(mul2(add2(fma2(R0, R1, Z), fma2(I0, I1, Z)), two), st[2][t], st[2][t + 1]);
+        unpack2(mul2(sub2(fma2(I0, R1, Z), fma2(R0, I1, Z)), two), st[3][t], st[3][t + 1]);
+    }
+}
+
 struct Item {
     int p, f, tc, b0;
 };
@@ -463,10 +485,34 @@ cb_kernel(const __grid_constant__ Params P)
             const int tile0 = it.tc * kTilesPerItem;
             const int tile1 = min(ntiles_gulp, tile0 + kTilesPerItem);
             bool ok = true;
+            constexpr int NC = STOKES == 4 ? 4 : 1;  // output components
+            // IB powers of this warp's outputs in the tile, fetched before the
+            // accumulator wait so that their latency hides behind it
+            constexpr int kEmits = kSlice / TS;
+            constexpr bool kPrefetch = kEmits * NC <= 4;
+            float ibp[kPrefetch ? kEmits * NC : 1];
             for(int tile = tile0; tile < tile1; ++tile) {
+                if constexpr(kPrefetch) {
+                    if(P.ib_subtract) {
+#pragma unroll
+                        for(int e = 0; e < kEmits; ++e) {
+                            const int to = (tile * kTileT + h * kSlice + (e + 1) * TS - 1) / TS;
+                            const size_t ii = ((size_t)bs * nout + to) * F + it.f;
+                            if constexpr(NC == 1) {
+                                ibp[e] = pr.ib_raw[ii];
+                            } else {
+                                const float4 v = reinterpret_cast<const float4*>(pr.ib_raw)[ii];
+                                ibp[4 * e] = v.x; ibp[4 * e + 1] = v.y;
+                                ibp[4 * e + 2] = v.z; ibp[4 * e + 3] = v.w;
+                            }
+                        }
+                    }
+                }
                 if(!mbar_wait(&acc_full[ab], aph, s_abort, deadline, P.err)) { ok = false; break; }
                 fence_after();
-                float power = 0.0f;  // carried across groups while tscrunch > 8
+                float power[NC];  // carried across groups while tscrunch > 8
+#pragma unroll
+                for(int c = 0; c < NC; ++c) power[c] = 0.0f;
 #pragma unroll
                 for(int g = 0; g < kGroups; ++g) {
                     const uint32_t ta = lane_base + ab * 256 + h * kSlice + g * 8;
@@ -487,26 +533,55 @@ cb_kernel(const __grid_constant__ Params P)
                                 make_int2((int)r1[t], (int)i1[t]);
                         }
                     }
-                    float st[8];
-                    stokes_n<STOKES, 8>(r0, r1, i0, i1, st);
+                    float st[NC][8];
+                    if constexpr(STOKES == 4) stokes_iquv<8>(r0, r1, i0, i1, st);
+                    else stokes_n<STOKES, 8>(r0, r1, i0, i1, st[0]);
 #pragma unroll
                     for(int t = 0; t < 8; ++t) {
-                        power = fadd(power, st[t]);
+#pragma unroll
+                        for(int c = 0; c < NC; ++c) power[c] = fadd(power[c], st[c][t]);
                         const int u = g * 8 + t;  // sample within this warp's slice
                         const bool emit = ((u + 1) % TS) == 0;
                         if(emit) {
                             const int to = (tbase + t) / TS;
-                            float v;
-                            if(P.ib_subtract) {
-                                const float ib = pr.ib_raw[((size_t)bs * nout + to) * F + it.f];
-                                v = rintf(fdiv(fsub(power, fmul(ib, 16129.0f)), scale));
-                            } else if(STOKES == 0) {
-                                v = rintf(fdiv(fsub(power, offs), scale));
+                            const size_t ii = ((size_t)bs * nout + to) * F + it.f;
+                            const size_t oi = ((size_t)to * F + it.f) * P.nbeams + b;
+                            const int e = u / TS;  // emit index within the slice
+                            if constexpr(NC == 1) {
+                                float v;
+                                if(P.ib_subtract) {
+                                    const float ib = kPrefetch ? ibp[kPrefetch ? e : 0] : pr.ib_raw[ii];
+                                    v = rintf(fdiv(fsub(power[0], fmul(ib, 16129.0f)), scale));
+                                } else if(STOKES == 0) {
+                                    v = rintf(fdiv(fsub(power[0], offs), scale));
+                                } else {
+                                    v = rintf(fdiv(power[0], scale));
+                                }
+                                if(valid) pr.out[oi] = clamp_i8(v);
                             } else {
-                                v = rintf(fdiv(power, scale));
+                                // char4 {I, Q, U, V}; the IB power is float4
+                                float v[4];
+                                if(P.ib_subtract) {
+                                    const float4 ib = kPrefetch
+                                        ? make_float4(ibp[0], ibp[1], ibp[2], ibp[3])
+                                        : reinterpret_cast<const float4*>(pr.ib_raw)[ii];
+                                    v[0] = rintf(fdiv(fsub(power[0], fmul(ib.x, 16129.0f)), scale));
+                                    v[1] = rintf(fdiv(fsub(power[1], fmul(ib.y, 16129.0f)), scale));
+                                    v[2] = rintf(fdiv(fsub(power[2], fmul(ib.z, 16129.0f)), scale));
+                                    v[3] = rintf(fdiv(fsub(power[3], fmul(ib.w, 16129.0f)), scale));
+                                } else {
+                                    v[0] = rintf(fdiv(fsub(power[0], offs), scale));
+                                    v[1] = rintf(fdiv(power[1], scale));
+                                    v[2] = rintf(fdiv(power[2], scale));
+                                    v[3] = rintf(fdiv(power[3], scale));
+                                }
+                                if(valid)
+                                    reinterpret_cast<char4*>(pr.out)[oi] =
+                                        make_char4(clamp_i8(v[0]), clamp_i8(v[1]),
+                                                   clamp_i8(v[2]), clamp_i8(v[3]));
                             }
-                            if(valid) pr.out[((size_t)to * F + it.f) * P.nbeams + b] = clamp_i8(v);
-                            power = 0.0f;
+#pragma unroll
+                            for(int c = 0; c < NC; ++c) power[c] = 0.0f;
                         }
                     }
                 }
@@ -627,7 +702,7 @@ int launch(const sw_cb_shape* s, const sw_cb_problem* probs, int nprob,
                "Number of samples must be a multiple of %d", kTileT);
     SW_REQUIRE(s->tscrunch >= 1 && s->tscrunch <= 32 && (s->tscrunch & (s->tscrunch - 1)) == 0,
                "CoherentBeamformer: tscrunch must be a power of two <= 32");
-    SW_REQUIRE(s->stokes >= 0 && s->stokes <= 3, "CoherentBeamformer: bad Stokes mode");
+    SW_REQUIRE(s->stokes >= 0 && s->stokes <= 4, "CoherentBeamformer: bad Stokes mode");
     SW_REQUIRE(s->row_stride % 16 == 0 && s->sample_offset % 16 == 0,
                "CoherentBeamformer: FPACT stride/offset must be multiples of 16");
     SW_REQUIRE(s->sample_offset + (size_t)s->nsamples <= s->row_stride,
@@ -644,6 +719,10 @@ int launch(const sw_cb_shape* s, const sw_cb_problem* probs, int nprob,
         const sw_cb_problem& pr = probs[i];
         SW_REQUIRE(pr.d_fpact && pr.d_out && (pr.d_ib_raw || !s->ib_subtract),
                    "CoherentBeamformer: problem %d has a null pointer", i);
+        SW_REQUIRE(s->stokes != 4 || ((reinterpret_cast<uintptr_t>(pr.d_out) & 3) == 0 &&
+                                      (reinterpret_cast<uintptr_t>(pr.d_ib_raw) & 15) == 0),
+                   "CoherentBeamformer: IQUV needs 4-byte aligned output and 16-byte aligned "
+                   "IB powers");
         SW_REQUIRE(pr.beam_start >= 0 && pr.beam_count > 0 &&
                        pr.beam_start + pr.beam_count <= s->nbeams,
                    "CoherentBeamformer: problem %d beam range out of bounds", i);
@@ -714,7 +793,8 @@ int dispatch_stokes(int stokes, int grid, size_t smem, cudaStream_t stream)
     case 0: return launch_variant<TS, 0>(grid, smem, stream);
     case 1: return launch_variant<TS, 1>(grid, smem, stream);
     case 2: return launch_variant<TS, 2>(grid, smem, stream);
-    default: return launch_variant<TS, 3>(grid, smem, stream);
+    case 3: return launch_variant<TS, 3>(grid, smem, stream);
+    default: return launch_variant<TS, 4>(grid, smem, stream);
     }
 }
 

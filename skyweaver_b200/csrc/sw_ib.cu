@@ -44,18 +44,23 @@ __device__ __forceinline__ float stokes_f(int stokes, float r0, float i0,
     }
 }
 
+// NC = 1: one Stokes parameter (args.stokes); NC = 4: I, Q, U, V
+// (FullStokesBeamformerTraits, beamformer_utils.cuh:198-278: float4 raw power,
+// char4 output, component c computed exactly like single-Stokes mode c).
+template <int NC>
 __global__ void __launch_bounds__(128)
 ib_k(IbArgs args, int bs0)
 {
-    __shared__ float sw[kMaxBs][kMaxAnt];
-    __shared__ int s_intw[kMaxBs];
-    const int nbs = min(kMaxBs, args.nbeamsets - bs0);
-    for(int i = threadIdx.x; i < kMaxBs * args.nant; i += blockDim.x) {
+    constexpr int kBs = kMaxBs / NC;  // beamsets per pass
+    __shared__ float sw[kBs][kMaxAnt];
+    __shared__ int s_intw[kBs];
+    const int nbs = min(kBs, args.nbeamsets - bs0);
+    for(int i = threadIdx.x; i < kBs * args.nant; i += blockDim.x) {
         const int s = i / args.nant, a = i % args.nant;
         sw[s][a] = (s < nbs) ? args.weights[(size_t)(bs0 + s) * args.nant + a] : 0.0f;
     }
     __syncthreads();
-    if(threadIdx.x < kMaxBs) {
+    if(threadIdx.x < kBs) {
         int ok = 1;
         for(int a = 0; a < args.nant; ++a) {
             const float w = sw[threadIdx.x][a];
@@ -71,9 +76,13 @@ ib_k(IbArgs args, int bs0)
     if(tp >= nout) return;
     const int t0 = tp * args.tscrunch;
     const size_t P = 2;
-    long long S[kMaxBs], B[kMaxBs];
+    long long S[kBs * NC], B[kBs];
 #pragma unroll
-    for(int s = 0; s < kMaxBs; ++s) { S[s] = 0; B[s] = 0; }
+    for(int s = 0; s < kBs; ++s) {
+        B[s] = 0;
+#pragma unroll
+        for(int c = 0; c < NC; ++c) S[s * NC + c] = 0;
+    }
 
     const bool words = (args.tscrunch % 4) == 0;
     for(int a = 0; a < args.nant; ++a) {
@@ -104,43 +113,51 @@ ib_k(IbArgs args, int bs0)
                 pV += xi0 * xr1 - xr0 * xi1;
             }
         }
-        const int pv = args.stokes == 0 ? pI : args.stokes == 1 ? pQ
-                     : args.stokes == 2 ? 2 * pU : 2 * pV;
+        int pv[NC];
+        if constexpr(NC == 4) {
+            pv[0] = pI; pv[1] = pQ; pv[2] = 2 * pU; pv[3] = 2 * pV;
+        } else {
+            pv[0] = args.stokes == 0 ? pI : args.stokes == 1 ? pQ
+                  : args.stokes == 2 ? 2 * pU : 2 * pV;
+        }
 #pragma unroll
-        for(int s = 0; s < kMaxBs; ++s) {
-            const float w = sw[s][a];
-            const int wi = (int)w;
-            S[s] += (long long)wi * pv;
+        for(int s = 0; s < kBs; ++s) {
+            const int wi = (int)sw[s][a];
+#pragma unroll
+            for(int c = 0; c < NC; ++c) S[s * NC + c] += (long long)wi * pv[c];
             B[s] += (long long)abs(wi) * pI;  // |Q|,|U|,|V| <= I per sample
         }
     }
 
     for(int s = 0; s < nbs; ++s) {
-        float power;
-        if(s_intw[s] && B[s] <= (1ll << 24)) {
-            power = (float)S[s];  // the float chain is exact
-        } else {
-            // reference order: t outer, a inner, float multiply and add
-            power = 0.0f;
-            for(int t = t0; t < t0 + args.tscrunch; ++t)
-                for(int a = 0; a < args.nant; ++a) {
-                    const uint8_t* q0 = args.fpact + (((size_t)f * P + 0) * args.nant + a) * 2 * args.row_stride + args.offset + t;
-                    const uint8_t* q1 = args.fpact + (((size_t)f * P + 1) * args.nant + a) * 2 * args.row_stride + args.offset + t;
-                    const float st = stokes_f(args.stokes, (float)(int8_t)q0[0],
-                                              (float)(int8_t)q0[args.row_stride],
-                                              (float)(int8_t)q1[0],
-                                              (float)(int8_t)q1[args.row_stride]);
-                    power = fadd(power, fmul(st, sw[s][a]));
-                }
-        }
         const int bs = bs0 + s;
         const size_t o  = ((size_t)bs * nout + tp) * args.nchans + f;
         const size_t so = (size_t)bs * args.nchans + f;
-        args.raw[o] = power;
-        const float sc = args.stokes == 0
-                             ? rintf(fdiv(fsub(power, args.offset_v[so]), args.scale[so]))
-                             : rintf(fdiv(power, args.scale[so]));
-        args.out[o] = clamp_i8(sc);
+        for(int c = 0; c < NC; ++c) {
+            const int stokes = NC == 4 ? c : args.stokes;
+            float power;
+            if(s_intw[s] && B[s] <= (1ll << 24)) {
+                power = (float)S[s * NC + c];  // the float chain is exact
+            } else {
+                // reference order: t outer, a inner, float multiply and add
+                power = 0.0f;
+                for(int t = t0; t < t0 + args.tscrunch; ++t)
+                    for(int a = 0; a < args.nant; ++a) {
+                        const uint8_t* q0 = args.fpact + (((size_t)f * P + 0) * args.nant + a) * 2 * args.row_stride + args.offset + t;
+                        const uint8_t* q1 = args.fpact + (((size_t)f * P + 1) * args.nant + a) * 2 * args.row_stride + args.offset + t;
+                        const float st = stokes_f(stokes, (float)(int8_t)q0[0],
+                                                  (float)(int8_t)q0[args.row_stride],
+                                                  (float)(int8_t)q1[0],
+                                                  (float)(int8_t)q1[args.row_stride]);
+                        power = fadd(power, fmul(st, sw[s][a]));
+                    }
+            }
+            args.raw[o * NC + c] = power;
+            const float sc = stokes == 0
+                                 ? rintf(fdiv(fsub(power, args.offset_v[so]), args.scale[so]))
+                                 : rintf(fdiv(power, args.scale[so]));
+            args.out[o * NC + c] = clamp_i8(sc);
+        }
     }
 }
 
@@ -160,7 +177,7 @@ int launch_incoherent_beamform(const void* d_fpact, size_t row_stride,
     SW_REQUIRE(nant > 0 && nant <= kMaxAnt, "sw_incoherent_beamform: bad antenna count");
     SW_REQUIRE(tscrunch > 0 && nsamples % tscrunch == 0,
                "sw_incoherent_beamform: nsamples must be a multiple of tscrunch");
-    SW_REQUIRE(stokes >= 0 && stokes <= 3, "sw_incoherent_beamform: bad Stokes mode");
+    SW_REQUIRE(stokes >= 0 && stokes <= 4, "sw_incoherent_beamform: bad Stokes mode");
     SW_REQUIRE(tscrunch % 4 != 0 || (row_stride % 4 == 0 && sample_offset % 4 == 0),
                "sw_incoherent_beamform: stride/offset must be multiples of 4");
     SW_REQUIRE(nchans > 0 && nchans <= 65535, "sw_incoherent_beamform: bad channel count");
@@ -169,9 +186,16 @@ int launch_incoherent_beamform(const void* d_fpact, size_t row_stride,
                 d_offset, d_beamset_weights, d_raw, d_out};
     const int nout = nsamples / tscrunch;
     dim3 grid(cdiv(nout, 128), nchans);
-    for(int bs0 = 0; bs0 < nbeamsets; bs0 += kMaxBs) {
-        ib_k<<<grid, 128, 0, stream>>>(args, bs0);
-        SW_LAUNCH_CHECK();
+    if(stokes == 4) {
+        for(int bs0 = 0; bs0 < nbeamsets; bs0 += kMaxBs / 4) {
+            ib_k<4><<<grid, 128, 0, stream>>>(args, bs0);
+            SW_LAUNCH_CHECK();
+        }
+    } else {
+        for(int bs0 = 0; bs0 < nbeamsets; bs0 += kMaxBs) {
+            ib_k<1><<<grid, 128, 0, stream>>>(args, bs0);
+            SW_LAUNCH_CHECK();
+        }
     }
     return SW_OK;
 }

@@ -119,8 +119,9 @@ def incoherent_beamform(fpact, nsamples, tscrunch, scale, offset, beamset_weight
                         offset_samples=0, stokes="I", stream=None):
     F, P, A, _, stride = fpact.shape
     S = beamset_weights.shape[0]
-    raw = torch.empty((S, nsamples // tscrunch, F), dtype=torch.float32, device=fpact.device)
-    out = torch.empty((S, nsamples // tscrunch, F), dtype=torch.int8, device=fpact.device)
+    shape = (S, nsamples // tscrunch, F) + ((4,) if stokes == "IQUV" else ())
+    raw = torch.empty(shape, dtype=torch.float32, device=fpact.device)
+    out = torch.empty(shape, dtype=torch.int8, device=fpact.device)
     call("sw_incoherent_beamform", _ptr(fpact), stride, offset_samples, F, nsamples, A,
          tscrunch, _ptr(scale), _ptr(offset), _ptr(beamset_weights), S, STOKES[stokes],
          _ptr(raw), _ptr(out), _stream(stream))
@@ -142,8 +143,8 @@ def coherent_beamform(fpact, weights_gemm, scale, offset, mapping, ib_raw, nsamp
     nbeams = weights_gemm.shape[2]
     beam_count = nbeams if beam_count is None else beam_count
     if out is None:
-        out = torch.zeros((nsamples // tscrunch, F, nbeams), dtype=torch.int8,
-                          device=fpact.device)
+        out = torch.zeros((nsamples // tscrunch, F, nbeams) + ((4,) if stokes == "IQUV" else ()),
+                          dtype=torch.int8, device=fpact.device)
     dbg = (torch.zeros((F, nsamples, 2, nbeams, 2), dtype=torch.int32, device=fpact.device)
            if debug else None)
     shape = cb_shape(fpact, nsamples, nbeams, tscrunch, stokes, ib_subtract, offset_samples)
@@ -206,11 +207,17 @@ class CoherentDedisperser:
 
 # ----------------------------------------------------- incoherent dedisp.
 def incoherent_dedisperse(tfb, delays, max_delay, tscrunch, scale_factor, stream=None):
-    T, F, B = tfb.shape
+    """IncoherentDedisperser::dedisperse: int8 TFB [T][F][B] -> TDB
+    [(T - max_delay) / tscrunch][D][B].  A char4 (IQUV) TFB [T][F][B][4] is
+    dedispersed per component (the reference's char4 instantiation,
+    IncoherentDedisperser.cu:133-137, sums and clamps each component
+    independently), i.e. as 4B int8 beams."""
+    T, F, B = tfb.shape[:3]
+    C = tfb.shape[3] if tfb.dim() == 4 else 1
     ndms = delays.shape[0]
-    out = torch.empty(((T - max_delay) // tscrunch, ndms, B), dtype=torch.int8,
-                      device=tfb.device)
-    call("sw_incoherent_dedisperse", _ptr(tfb), T, F, B, _ptr(delays), ndms, max_delay,
+    out = torch.empty(((T - max_delay) // tscrunch, ndms, B) + ((C,) if tfb.dim() == 4 else ()),
+                      dtype=torch.int8, device=tfb.device)
+    call("sw_incoherent_dedisperse", _ptr(tfb), T, F, B * C, _ptr(delays), ndms, max_delay,
          tscrunch, ctypes.c_float(scale_factor), _ptr(out), _stream(stream))
     return out
 
@@ -241,6 +248,7 @@ class BeamformerPipeline:
         self.nchans, self.nbeams, self.tscrunch, self.gulp = nchans, nbeams, tscrunch, gulp_samples
         self.nbeamsets = bw.shape[0]
         self._nant = nantennas
+        self.stokes = stokes
 
     def close(self):
         if self.h:
@@ -283,10 +291,11 @@ class BeamformerPipeline:
         torch.cuda.synchronize()
         T = self.gulp // self.tscrunch
         S, F, B = self.nbeamsets, self.nchans, self.nbeams
+        C = (4,) if self.stokes == "IQUV" else ()
         res = {}
-        for name, p, dt, shape in (("cb", pcb, np.int8, (T, F, B)),
-                                   ("ib_raw", praw, np.float32, (S, T, F)),
-                                   ("ib", pib, np.int8, (S, T, F)),
+        for name, p, dt, shape in (("cb", pcb, np.int8, (T, F, B) + C),
+                                   ("ib_raw", praw, np.float32, (S, T, F) + C),
+                                   ("ib", pib, np.int8, (S, T, F) + C),
                                    ("stats", pst, np.float32, (F, 2, -1, 4))):
             n = int(np.prod([x for x in shape if x > 0]))
             if name == "stats":

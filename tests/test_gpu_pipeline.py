@@ -120,6 +120,7 @@ def test_ragged_beamsets_grouped_equals_plain_and_oracle(cuda, oracle):
                                          bandwidth=bw, dms=dms, beamset_weights=masks,
                                          beamset_mapping=mapping, **kw)
         pipe.set_delays(delays, 1.7e9)
+        fft_len, overlap = pipe.fft_plan()
         pipe.process_device(torch.from_numpy(taftp).cuda(), 1.7e9)
         outs[name] = [pipe.outputs(d) for d in range(len(dms))]
         pipe.close()
@@ -130,5 +131,43 @@ def test_ragged_beamsets_grouped_equals_plain_and_oracle(cuda, oracle):
     scl = oracle.scalings(oracle.statistics(ftpa), masks, len(beams), ts, ts, 24.0)
     freqs = synthetic.channel_frequencies(centre, bw, F)
     w = oracle.weights(delays, freqs, 1.7e9, 1.7e9)
-    cb_ref = oracle.coherent_beam(ftpa, w, ts, scl[1], scl[0], masks, mapping)
+    # first gulp: zero history, DM 0 output delayed by overlap / 2
+    ext = np.concatenate([np.zeros((F, overlap, 2, A, 2), np.int8), ftpa], axis=1)
+    low = float(np.float32(centre - bw / 2))
+    dd = oracle.cdd_ftpa(ext, T, oracle.chirp(F, fft_len, low, bw, 0.0), overlap)
+    cb_ref = oracle.coherent_beam(dd, w, ts, scl[1], scl[0], masks, mapping)
     assert np.array_equal(outs["grouped"][0]["cb"], cb_ref)
+
+
+def test_pipeline_full_stokes_iquv(cuda, oracle):
+    """Stokes IQUV through the pipeline: char4 coherent beams, float4/char4
+    incoherent beams, DM 0 bit-identical to the oracle chain."""
+    torch = cuda
+    from skyweaver_b200 import stages, synthetic
+    g = synthetic.rng(78)
+    A, F, B, T, ts = 32, 2, 128, 2048, 8
+    chbw = 856e6 / 1024
+    centre, bw = 1284e6, F * chbw
+    mapping = np.zeros(B, np.int32)
+    mapping[70:] = 1
+    masks = synthetic.beamset_masks(g, A, [32, 20])
+    delays = synthetic.delay_model(g, B, A)
+    delays[..., 0] = masks[mapping]
+    pipe = stages.BeamformerPipeline(nantennas=A, input_nantennas=A, nchans=F, nbeams=B,
+                                     gulp_samples=T, tscrunch=ts, centre_frequency=centre,
+                                     bandwidth=bw, dms=[0.0], beamset_weights=masks,
+                                     beamset_mapping=mapping, stokes="IQUV")
+    pipe.set_delays(delays, 1.7e9)
+    taftp = synthetic.voltages_taftp(g, T // 256, A, F, sigma=8)
+    pipe.process_device(torch.from_numpy(taftp).cuda(), 1.7e9)
+    out = pipe.outputs(0)
+    pipe.close()
+    ftpa = oracle.transpose(taftp, A)
+    scl = oracle.scalings(oracle.statistics(ftpa), masks, 2, ts, ts, 24.0)
+    w = oracle.weights(delays, synthetic.channel_frequencies(centre, bw, F), 1.7e9, 1.7e9)
+    raw_ref, ib_ref = oracle.incoherent_beam(ftpa, ts, scl[3], scl[2], masks, 2, "IQUV")
+    cb_ref = oracle.coherent_beam(ftpa, w, ts, scl[1], scl[0], masks, mapping, "IQUV")
+    assert out["cb"].shape == (T // ts, F, B, 4)
+    assert np.array_equal(out["ib_raw"], raw_ref)
+    assert np.array_equal(out["ib"], ib_ref)
+    assert np.array_equal(out["cb"], cb_ref)

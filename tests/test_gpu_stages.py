@@ -117,7 +117,7 @@ def test_weights(cuda, oracle, case):
 
 
 # ----------------------------------------------------- incoherent beam
-@pytest.mark.parametrize("stokes", ["I", "Q", "U", "V"])
+@pytest.mark.parametrize("stokes", ["I", "Q", "U", "V", "IQUV"])
 @pytest.mark.parametrize("nbeamsets", [1, 4])
 def test_incoherent_beam_bit_exact(cuda, oracle, stokes, nbeamsets):
     from skyweaver_b200 import stages, synthetic
@@ -139,7 +139,8 @@ def test_incoherent_beam_bit_exact(cuda, oracle, stokes, nbeamsets):
     assert np.array_equal(_np(out), out_ref)
 
 
-def test_incoherent_beam_float_chain_path(cuda, oracle):
+@pytest.mark.parametrize("stokes", ["I", "IQUV"])
+def test_incoherent_beam_float_chain_path(cuda, oracle, stokes):
     """Strong RFI and non-integer weights force the reference-order float chain."""
     from skyweaver_b200 import stages, synthetic
     g = synthetic.rng(12)
@@ -150,10 +151,10 @@ def test_incoherent_beam_float_chain_path(cuda, oracle):
     bw = np.stack([np.ones(A, np.float32), g.uniform(0.3, 1.0, A).astype(np.float32)])
     scale = np.full(2 * F, 5000.0, np.float32)
     offset = np.full(2 * F, 1e5, np.float32)
-    raw_ref, out_ref = oracle.incoherent_beam(ftpa, ts, scale, offset, bw, 2)
+    raw_ref, out_ref = oracle.incoherent_beam(ftpa, ts, scale, offset, bw, 2, stokes)
     fp = stages.transpose_fpact(_dev(cuda, taftp), A)
     raw, out = stages.incoherent_beamform(fp, H * 256, ts, _dev(cuda, scale),
-                                          _dev(cuda, offset), _dev(cuda, bw))
+                                          _dev(cuda, offset), _dev(cuda, bw), stokes=stokes)
     assert np.array_equal(_np(raw), raw_ref)
     assert np.array_equal(_np(out), out_ref)
 
@@ -206,7 +207,7 @@ def _report(out, ref):
     return "\n".join(lines)
 
 
-@pytest.mark.parametrize("stokes", ["I", "Q", "U", "V"])
+@pytest.mark.parametrize("stokes", ["I", "Q", "U", "V", "IQUV"])
 @pytest.mark.parametrize("ib_sub", [True, False])
 def test_coherent_beam_stokes(cuda, oracle, stokes, ib_sub):
     out, ref, dbg, volts = _cb_case(cuda, oracle, 64, 256, 3, 2, 4, stokes, ib_sub, seed=22)
@@ -335,3 +336,23 @@ def test_incoherent_dedispersion_ones(cuda, oracle):
                                            float(np.float32(math.sqrt(F * ts)))))
     assert got.shape == ((T - maxd) // ts, 5, B)
     assert np.all(got == int(math.sqrt(F * ts)))
+
+
+def test_incoherent_dedispersion_char4_iquv(cuda, oracle):
+    """char4 (IQUV) TFB: every component dedispersed and clamped on its own,
+    like the reference's char4 instantiation (IncoherentDedisperser.cu:133-137)."""
+    from skyweaver_b200 import stages, synthetic
+    g = synthetic.rng(42)
+    F, B, ts = 32, 16, 4
+    freqs = synthetic.channel_frequencies(1284e6, 32 * 856e6 / 1024, F)
+    dms = np.array([0, 50, 100], np.float32)
+    delays, maxd = oracle.idd_delays(freqs, dms, ts * 16 / (856e6 / 1024))
+    T = maxd + 32 * ts
+    tfb = g.integers(-128, 128, size=(T, F, B, 4), dtype=np.int8)
+    sf = np.float32(math.sqrt(F * ts))
+    got = _np(stages.incoherent_dedisperse(_dev(cuda, tfb), _dev(cuda, delays), maxd, ts,
+                                           float(sf)))
+    assert got.shape == ((T - maxd) // ts, 3, B, 4)
+    for c in range(4):
+        ref = oracle.idd(np.ascontiguousarray(tfb[..., c]), delays, maxd, ts, sf)
+        assert np.array_equal(got[..., c], ref)
