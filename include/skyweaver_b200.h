@@ -223,7 +223,7 @@ int sw_coherent_beamform_grouped(const sw_cb_shape* shape,
 /* ------------------------------------------------------------------ */
 /* Bytes of the device setup block (per-pass FFT twiddle tables followed by
  * the chirp tables) for sw_cdd_chirps / sw_coherent_dedisperse; 0 if
- * fft_len is not a supported power of two (256 .. 8192). */
+ * fft_len is not a supported power of two (256 .. 65536). */
 size_t sw_cdd_setup_bytes(int ndms, int nchans, int fft_len);
 
 /* Replaces create_coherent_dedisperser_config's response tables, i.e.
@@ -249,6 +249,27 @@ int sw_coherent_dedisperse(const void* d_fpact_in, size_t row_stride,
                            int fft_len, int overlap, const void* d_setup,
                            int ndms, void* const* h_d_out,
                            size_t out_row_stride, sw_stream_t stream);
+
+/* Workspace bytes sw_coherent_dedisperse_ws needs to process every
+ * overlap-save segment of a gulp in one pass (0 for fft_len <= 8192, which
+ * runs entirely on chip). fft_len 16384, 32768 and 65536 are split into
+ * 8192-point sub-transforms whose intermediate spectra pass through this
+ * complex workspace. */
+size_t sw_cdd_workspace_bytes(int nchans, int npol, int nant, int nsamples,
+                              int fft_len, int overlap, int ndms);
+
+/* sw_coherent_dedisperse for any fft_len in [256, 65536]. A workspace
+ * smaller than sw_cdd_workspace_bytes is used in chunks of segments (at
+ * least ndms * fft_len * 8 bytes). d_debug_f32, if not null, receives the
+ * dedispersed voltages before rounding: float2 [ndms][nchans][npol][nant]
+ * [nsamples] (re, im), for precision studies against an FP64 reference. */
+int sw_coherent_dedisperse_ws(const void* d_fpact_in, size_t row_stride,
+                              int nchans, int npol, int nant, int nsamples,
+                              int fft_len, int overlap, const void* d_setup,
+                              int ndms, void* const* h_d_out,
+                              size_t out_row_stride, void* d_workspace,
+                              size_t workspace_bytes, float* d_debug_f32,
+                              sw_stream_t stream);
 
 /* ------------------------------------------------------------------ */
 /* IncoherentDedisperser                                                */

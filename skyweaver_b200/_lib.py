@@ -90,6 +90,10 @@ _SIGS = {
     "sw_coherent_dedisperse": (c_int, [c_void_p, c_size_t, c_int, c_int, c_int, c_int, c_int,
                                        c_int, c_void_p, c_int, ctypes.POINTER(c_void_p),
                                        c_size_t, c_void_p]),
+    "sw_cdd_workspace_bytes": (c_size_t, [c_int, c_int, c_int, c_int, c_int, c_int, c_int]),
+    "sw_coherent_dedisperse_ws": (c_int, [c_void_p, c_size_t, c_int, c_int, c_int, c_int, c_int,
+                                          c_int, c_void_p, c_int, ctypes.POINTER(c_void_p),
+                                          c_size_t, c_void_p, c_size_t, c_void_p, c_void_p]),
     "sw_incoherent_dedisperse": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_int,
                                          c_int, c_int, c_float, c_void_p, c_void_p]),
     "sw_pipeline_create": (c_int, [ctypes.POINTER(PipelineConfig), ctypes.POINTER(c_void_p)]),

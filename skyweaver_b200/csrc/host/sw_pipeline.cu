@@ -13,6 +13,7 @@
 // pair.  process_host double-buffers the pinned-host input and the outputs
 // so that the H2D of gulp g+1 and the D2H of gulp g-1 overlap the compute
 // of gulp g on separate copy streams.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -76,7 +77,7 @@ struct sw_pipeline {
     std::vector<DevBuf> dd;
     DevBuf stats, stats_scratch;
     DevBuf cb_off, cb_scl, ib_off, ib_scl;
-    DevBuf d_bw, d_map, d_delays, d_freqs, d_wgemm, d_setup;
+    DevBuf d_bw, d_map, d_delays, d_freqs, d_wgemm, d_setup, cdd_ws;
     DevBuf epochs;  // [2 parities][2] doubles
     std::vector<DevBuf> ib_raw[2], ib_i8[2], cb[2];
     double* h_epochs = nullptr;  // pinned [2][2]
@@ -159,8 +160,9 @@ int sw_pipeline::init(const sw_pipeline_config& c)
                 if(cost < best - 1e-9) { best = cost; fft_len = n; }
             }
         }
-        SW_REQUIRE(fft_len > overlap && fft_len >= 256 && fft_len <= 8192,
-                   "pipeline: DM smear of %d samples needs an FFT longer than 8192", overlap);
+        SW_REQUIRE(fft_len > overlap && fft_len >= 256 && fft_len <= 65536,
+                   "pipeline: fft_len %d does not exceed the DM smear of %d samples or is "
+                   "outside [256, 65536]", fft_len, overlap);
         SW_REQUIRE(T >= overlap, "pipeline: gulp shorter than the dedispersion overlap");
     } else {
         overlap = 0;
@@ -191,6 +193,13 @@ int sw_pipeline::init(const sw_pipeline_config& c)
         dd.resize(ndm);
         for(int d = 0; d < ndm; ++d) SW_TRY(dd[d].alloc(nrows * dd_stride));
         SW_TRY(d_setup.alloc(sw_cdd_setup_bytes(ndm, F, fft_len)));
+        // long FFTs (> 8192) pass their sub-transform spectra through a
+        // workspace: at most 4 GiB, processed in chunks of segments
+        const size_t ws = sw_cdd_workspace_bytes(F, 2, A, T, fft_len, overlap, ndm);
+        if(ws) {
+            const size_t per_seg = (size_t)ndm * fft_len * 8;
+            SW_TRY(cdd_ws.alloc(std::max(per_seg, std::min(ws, (size_t)4 << 30) / per_seg * per_seg)));
+        }
         const double low = (double)(float)(c.centre_frequency - c.bandwidth / 2.0f);
         SW_TRY(sw_cdd_chirps(dms.data(), ndm, F, fft_len, low, c.bandwidth, d_setup.p,
                              (sw_stream_t)compute));
@@ -246,8 +255,9 @@ int sw_pipeline::enqueue_chain(const void* d_in, int parity, bool first)
     if(cfg.enable_coherent_dedispersion) {
         std::vector<void*> outs(ndm);
         for(int d = 0; d < ndm; ++d) outs[d] = dd[d].p;
-        SW_TRY(sw_coherent_dedisperse(ext.p, ext_stride, F, 2, A, T, fft_len, overlap,
-                                      d_setup.p, ndm, outs.data(), dd_stride, ss));
+        SW_TRY(sw_coherent_dedisperse_ws(ext.p, ext_stride, F, 2, A, T, fft_len, overlap,
+                                         d_setup.p, ndm, outs.data(), dd_stride, cdd_ws.p,
+                                         cdd_ws.n, nullptr, ss));
         SW_TRY(sw_fpact_keep_history(ext.p, nrows, ext_stride, (size_t)overlap, ss));
         for(int d = 0; d < ndm; ++d) volt[d] = dd[d].p;
         vstride = dd_stride;

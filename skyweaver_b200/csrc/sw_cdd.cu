@@ -21,6 +21,8 @@
 // no spectrum in HBM, and all global traffic is coalesced byte rows.
 // Twiddles come from per-pass tables (FP64-computed) staged in shared
 // memory; FFT arithmetic is FP32.
+#include <algorithm>
+
 #include "sw_common.cuh"
 
 namespace swb {
@@ -215,6 +217,7 @@ struct Args {
     int npa;           // P * A (streams per channel)
     uint8_t* out[kMaxDms];
     size_t out_stride;
+    float2* dbg;  // optional [ndms][nstreams][nsamples] scaled values before rounding
 };
 
 // Twiddles w[1..R-1] of butterfly column j for a pass with stride s.
@@ -338,7 +341,7 @@ __device__ __forceinline__ void stage_input(uint8_t* st, const Args& A, int item
 
 // at least two resident CTAs per SM below N = 8192 (latency hiding across
 // the per-pass barriers); N = 8192 needs 512 threads and fits one.
-template <int LOGN>
+template <int LOGN, bool DBG>
 __global__ void __launch_bounds__((1 << LOGN) / 16, LOGN >= 13 ? 1 : (LOGN == 12 ? 2 : 4))
 cdd_kernel(const __grid_constant__ Args A)
 {
@@ -458,10 +461,12 @@ cdd_kernel(const __grid_constant__ Args A)
                     const int i = j + r * s0;           // index within the window
                     const int m = start + i - half;     // output sample in the gulp
                     if(i >= half && i < half + L && m < A.nsamples) {
-                        const int vr = __float2int_rn(z[r].x * inv_n);
-                        const int vi = __float2int_rn(z[r].y * inv_n);
-                        o_re[m] = (uint8_t)vr;  // int8 wrap, like static_cast<char>
-                        o_im[m] = (uint8_t)vi;
+                        const float fr = z[r].x * inv_n, fi = z[r].y * inv_n;
+                        o_re[m] = (uint8_t)__float2int_rn(fr);  // int8 wrap, like static_cast<char>
+                        o_im[m] = (uint8_t)__float2int_rn(fi);
+                        if constexpr(DBG)
+                            A.dbg[((size_t)d * A.nstreams + stream) * A.nsamples + m] =
+                                make_float2(fr, fi);
                     }
                 }
             }
@@ -469,6 +474,220 @@ cdd_kernel(const __grid_constant__ Args A)
         }
     }
     asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
+// ------------------------------------------------- long FFTs (N = S x 8192)
+// Overlap-save windows longer than one CTA's shared memory are split four-step
+// style into S = N / 8192 sub-transforms of M = 8192 points:
+//   n = M n1 + n2, k = k1 + S k2 (n1, k1 < S; n2, k2 < M)
+//   forward:  X[k1 + S k2] = DFT_M over n2 of
+//                 W_N^(n2 k1) * sum_n1 x[M n1 + n2] W_S^(n1 k1)
+//   inverse:  x[n2 + M n1] = sum_k1 W_S^(-n1 k1) *
+//                 W_N^(-n2 k1) * IDFT_M over k2 of Y[k1 + S k2]
+// cdd_split_kernel runs one (segment, k1) per CTA: the S-point partial DFT
+// straight from the int8 rows, the M-point forward FFT, and for every DM the
+// chirp of bins k1 + S k2 and the M-point inverse FFT, leaving
+// W_N^(-n2 k1) * z in a complex workspace; cdd_split_combine then does the
+// S-point inverse DFT over k1, the overlap-save trim, /N, rint and int8 wrap.
+constexpr int kSplitLog = 13;
+constexpr int kSplitM   = 1 << kSplitLog;
+
+struct SplitArgs {
+    const uint8_t* in;
+    size_t row_stride;
+    int nstreams, nsamples, overlap, nseg, ndms, npa;
+    int item0, nitems;  // work items [item0, item0 + nitems) of this chunk
+    const c32* tw;      // M-point plan tables
+    const c32* chirp;   // [ndms][F][S][M]: bin k1 + S k2 at k1's per-thread load order
+    const c32* tws;     // [S][M]: W_N^(n2 k1)
+    c32* z;             // [ndms][nitems][S][M]
+    uint8_t* out[kMaxDms];
+    size_t out_stride;
+    float2* dbg;
+};
+
+// W_S^m (forward sign) for S in {2, 4, 8}
+template <int S>
+__device__ __forceinline__ c32 wsm(int m)
+{
+    const float c2 = 0.70710678118654752440f;
+    switch((m % S) * (8 / S)) {
+    case 0: return {1.0f, 0.0f};
+    case 1: return {c2, -c2};
+    case 2: return {0.0f, -1.0f};
+    case 3: return {-c2, -c2};
+    case 4: return {-1.0f, 0.0f};
+    case 5: return {-c2, c2};
+    case 6: return {0.0f, 1.0f};
+    default: return {c2, c2};
+    }
+}
+
+template <int S>
+__global__ void __launch_bounds__(kSplitM / 16, 1)
+cdd_split_kernel(const __grid_constant__ SplitArgs A)
+{
+    constexpr int LOGN = kSplitLog;
+    constexpr int M  = kSplitM;
+    constexpr int N  = S * M;
+    constexpr int NT = M / 16;
+    constexpr Plan P = make_plan(LOGN);
+    constexpr int R0 = P.r0;
+    constexpr int B0 = 16 / R0;
+    extern __shared__ __align__(16) uint8_t smem[];
+    c32* buf  = reinterpret_cast<c32*>(smem);
+    c32* tw_s = buf + pad(M) + 16;
+    for(int i = threadIdx.x; i < P.tw_total; i += NT) tw_s[i] = A.tw[i];
+    const int L = N - A.overlap;
+    const int avail = A.overlap + A.nsamples;
+
+    for(int u = blockIdx.x; u < A.nitems * S; u += gridDim.x) {
+        const int il = u / S, k1 = u - il * S;
+        const int item   = A.item0 + il;
+        const int stream = item / A.nseg;
+        const int seg    = item - stream * A.nseg;
+        const int f      = stream / A.npa;
+        const int start  = seg * L;
+        const int8_t* row_re = reinterpret_cast<const int8_t*>(A.in) + (size_t)stream * 2 * A.row_stride;
+        const int8_t* row_im = row_re + A.row_stride;
+        __syncthreads();  // previous unit's last reads of buf are done
+        // ---- S-point partial DFT for this k1, times W_N^(n2 k1)
+#pragma unroll 4
+        for(int v = 0; v < 16; ++v) {
+            const int n2 = threadIdx.x + v * NT;
+            c32 acc{0.0f, 0.0f};
+#pragma unroll
+            for(int n1 = 0; n1 < S; ++n1) {
+                const int idx = start + n1 * M + n2;
+                const c32 x = idx < avail ? c32{(float)row_re[idx], (float)row_im[idx]}
+                                          : c32{0.0f, 0.0f};
+                acc = cadd(acc, cmul(x, wsm<S>(n1 * k1)));
+            }
+            buf[pad(n2)] = cmul(acc, A.tws[(size_t)k1 * M + n2]);
+        }
+        __syncthreads();
+        // ---- M-point forward FFT (DIF) in shared memory
+        fwd_pass<LOGN, R0>(buf, tw_s, P.span[0], P.stride[0], P.tw_off[0]);
+        __syncthreads();
+#pragma unroll
+        for(int p = 1; p < P.npass - 1; ++p) {
+            fwd_pass<LOGN, 16>(buf, tw_s, P.span[p], P.stride[p], P.tw_off[p]);
+            __syncthreads();
+        }
+        c32 spec[16];
+#pragma unroll
+        for(int r = 0; r < 16; ++r) spec[r] = buf[pad(threadIdx.x * 16 + r)];
+        dft16<false>(spec);
+        const size_t chirp_dm = (size_t)(A.nstreams / A.npa) * N;  // complex per DM
+        const float4* chp = reinterpret_cast<const float4*>(A.chirp + (size_t)f * N + (size_t)k1 * M) + threadIdx.x;
+        __syncthreads();
+        for(int d = 0; d < A.ndms; ++d) {
+            const float4* cd = chp + (size_t)d * chirp_dm / 2;
+            c32 y[16];
+#pragma unroll
+            for(int k = 0; k < 8; ++k) {
+                const float4 c = cd[k * NT];
+                y[2 * k]     = cmul(spec[2 * k], c32{c.x, c.y});
+                y[2 * k + 1] = cmul(spec[2 * k + 1], c32{c.z, c.w});
+            }
+            dft16<true>(y);
+#pragma unroll
+            for(int r = 0; r < 16; ++r) buf[pad(threadIdx.x * 16 + r)] = y[r];
+            __syncthreads();
+#pragma unroll
+            for(int p = P.npass - 2; p >= 1; --p) {
+                inv_pass<LOGN, 16>(buf, tw_s, P.span[p], P.stride[p], P.tw_off[p]);
+                __syncthreads();
+            }
+            // last inverse pass, then W_N^(-n2 k1), to the workspace
+            c32* zo = A.z + (((size_t)d * A.nitems + il) * S + k1) * M;
+            constexpr int s0 = M / R0;
+#pragma unroll
+            for(int v = 0; v < B0; ++v) {
+                const int j = threadIdx.x + v * NT;
+                c32 z[R0];
+#pragma unroll
+                for(int q = 0; q < R0; ++q) z[q] = buf[pad(j + q * s0)];
+                {
+                    c32 w[R0];
+                    load_tw<R0>(tw_s, P.tw_off[0], s0, j, w);
+#pragma unroll
+                    for(int q = 1; q < R0; ++q) z[q] = cmulc(z[q], w[q]);
+                }
+                dft<R0, true>(z);
+#pragma unroll
+                for(int r = 0; r < R0; ++r) {
+                    const int n2 = j + r * s0;
+                    zo[n2] = cmulc(z[r], A.tws[(size_t)k1 * M + n2]);
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+template <int S>
+__global__ void __launch_bounds__(256)
+cdd_split_combine(const __grid_constant__ SplitArgs A)
+{
+    constexpr int M = kSplitM, N = S * M;
+    const int L = N - A.overlap, half = A.overlap / 2;
+    const float inv_n = 1.0f / (float)N;  // exact (power of two)
+    const size_t total = (size_t)A.ndms * A.nitems * M;
+    for(size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
+        idx += (size_t)gridDim.x * blockDim.x) {
+        const int n2 = (int)(idx % M);
+        const size_t rest = idx / M;
+        const int il = (int)(rest % A.nitems);
+        const int d  = (int)(rest / A.nitems);
+        const int item   = A.item0 + il;
+        const int stream = item / A.nseg;
+        const int seg    = item - stream * A.nseg;
+        const int start  = seg * L;
+        const c32* zi = A.z + ((size_t)d * A.nitems + il) * S * M + n2;
+        c32 z[S];
+#pragma unroll
+        for(int k1 = 0; k1 < S; ++k1) z[k1] = zi[(size_t)k1 * M];
+        dft<S, true>(z);  // z[n1] = sum_k1 W_S^(-n1 k1) z'[k1]
+        uint8_t* o_re = A.out[d] + (size_t)stream * 2 * A.out_stride;
+        uint8_t* o_im = o_re + A.out_stride;
+#pragma unroll
+        for(int n1 = 0; n1 < S; ++n1) {
+            const int i = n2 + n1 * M;
+            const int m = start + i - half;
+            if(i >= half && i < half + L && m < A.nsamples) {
+                const float fr = z[n1].x * inv_n, fi = z[n1].y * inv_n;
+                o_re[m] = (uint8_t)__float2int_rn(fr);
+                o_im[m] = (uint8_t)__float2int_rn(fi);
+                if(A.dbg)
+                    A.dbg[((size_t)d * A.nstreams + stream) * A.nsamples + m] = make_float2(fr, fi);
+            }
+        }
+    }
+}
+
+template <int S>
+int launch_split(SplitArgs a, int total_items, size_t ws_items, cudaStream_t stream)
+{
+    constexpr Plan P = make_plan(kSplitLog);
+    const size_t smem = (size_t)(pad(kSplitM) + 16 + ((P.tw_total + 1) & ~1)) * sizeof(c32);
+    SW_CUDA_CHECK(cudaFuncSetAttribute(cdd_split_kernel<S>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    for(int i0 = 0; i0 < total_items; i0 += (int)ws_items) {
+        a.item0  = i0;
+        a.nitems = (int)std::min<size_t>(ws_items, (size_t)(total_items - i0));
+        const long units = (long)a.nitems * S;
+        cdd_split_kernel<S><<<(int)std::min<long>(units, nsm), kSplitM / 16, smem, stream>>>(a);
+        SW_LAUNCH_CHECK();
+        const size_t total = (size_t)a.ndms * a.nitems * kSplitM;
+        const size_t blocks = std::min<size_t>(cdiv(total, (size_t)256), (size_t)nsm * 16);
+        cdd_split_combine<S><<<(int)blocks, 256, 0, stream>>>(a);
+        SW_LAUNCH_CHECK();
+    }
+    return SW_OK;
 }
 
 // ------------------------------------------------------------- setup
@@ -531,25 +750,71 @@ __global__ void chirp_k(c32* chirp, SetupArgs S)
     }
 }
 
-template <int LOGN>
-int launch_logn(const Args& a, cudaStream_t stream)
+// Chirp tables for the split transform: bin k1 + S k2 of sub-transform k1
+// at k1 * M + (the M-point per-thread load order of k2).
+__global__ void chirp_split_k(c32* chirp, SetupArgs S, int split)
+{
+    const Plan P = make_plan(kSplitLog);
+    const int nt = kSplitM / 16;
+    const int n  = split * kSplitM;
+    const size_t total = (size_t)S.ndms * S.nchans * n;
+    for(size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total;
+        i += (size_t)gridDim.x * blockDim.x) {
+        const int q  = (int)(i % n);
+        const int c  = (int)((i / n) % S.nchans);
+        const int d  = (int)(i / ((size_t)n * S.nchans));
+        const int k1 = q / kSplitM, qq = q % kSplitM;
+        const int t  = (qq >> 1) % nt;
+        const int r  = 2 * ((qq >> 1) / nt) + (qq & 1);
+        const int k  = k1 + split * digit_reverse(P, 16 * t + r);
+        const double nu0   = S.low_freq + c * S.coarse_bw - 0.5 * S.coarse_bw;
+        const double nu    = k * S.fine_bw;
+        const double phase = (nu * nu * S.prefactor[d]) / ((nu0 + nu) * nu0 * nu0);
+        double sn, cs;
+        sincos(phase, &sn, &cs);
+        chirp[i] = c32{(float)cs, (float)sn};
+    }
+}
+
+// W_N^(n2 k1) = exp(-2 pi i n2 k1 / N) in FP64, [k1][n2]
+__global__ void split_twiddle_k(c32* tws, int split)
+{
+    const int n = split * kSplitM;
+    for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int k1 = i / kSplitM, n2 = i % kSplitM;
+        double sn, cs;
+        sincospi(-2.0 * (double)((long long)n2 * k1) / (double)n, &sn, &cs);
+        tws[i] = c32{(float)cs, (float)sn};
+    }
+}
+
+template <int LOGN, bool DBG>
+int launch_logn_dbg(const Args& a, cudaStream_t stream)
 {
     constexpr int N = 1 << LOGN;
     constexpr Plan P = make_plan(LOGN);
     const size_t smem = (size_t)(pad(N) + 16 + ((P.tw_total + 1) & ~1)) * sizeof(c32) + 2 * N;
-    SW_CUDA_CHECK(cudaFuncSetAttribute(cdd_kernel<LOGN>,
+    SW_CUDA_CHECK(cudaFuncSetAttribute(cdd_kernel<LOGN, DBG>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int dev = 0, nsm = 148, per_sm = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    SW_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cdd_kernel<LOGN>,
+    SW_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cdd_kernel<LOGN, DBG>,
                                                                  N / 16, smem));
     if(per_sm < 1) per_sm = 1;
     const long items = (long)a.nstreams * a.nseg;
     const long grid  = items < (long)nsm * per_sm ? items : (long)nsm * per_sm;
-    cdd_kernel<LOGN><<<(int)grid, N / 16, smem, stream>>>(a);
+    cdd_kernel<LOGN, DBG><<<(int)grid, N / 16, smem, stream>>>(a);
     SW_LAUNCH_CHECK();
     return SW_OK;
+}
+
+// the float output for precision studies is a separate instance, so the
+// production kernel carries none of its registers
+template <int LOGN>
+int launch_logn(const Args& a, cudaStream_t stream)
+{
+    return a.dbg ? launch_logn_dbg<LOGN, true>(a, stream) : launch_logn_dbg<LOGN, false>(a, stream);
 }
 
 int log2_exact(int n)
@@ -570,22 +835,25 @@ extern "C" {
 size_t sw_cdd_setup_bytes(int ndms, int nchans, int fft_len)
 {
     const int logn = log2_exact(fft_len);
-    if(logn < 0) return 0;
-    const Plan P = make_plan(logn);
-    return ((size_t)P.tw_total + 16 + (size_t)ndms * nchans * fft_len) * sizeof(c32);
+    if(logn < 8 || logn > 16 || ndms <= 0 || nchans <= 0) return 0;
+    const Plan P = make_plan(logn > kSplitLog ? kSplitLog : logn);
+    const size_t split_tw = logn > kSplitLog ? (size_t)fft_len : 0;
+    return ((size_t)P.tw_total + 16 + (size_t)ndms * nchans * fft_len + split_tw) * sizeof(c32);
 }
 
 int sw_cdd_chirps(const float* h_dms, int ndms, int nchans, int fft_len,
                   double low_freq, double bw, void* d_setup, sw_stream_t stream)
 {
     const int logn = log2_exact(fft_len);
-    SW_REQUIRE(logn >= 8 && logn <= 13, "coherent dedispersion: fft_len must be a power of two in [256, 8192]");
+    SW_REQUIRE(logn >= 8 && logn <= 16,
+               "coherent dedispersion: fft_len must be a power of two in [256, 65536]");
     SW_REQUIRE(h_dms && ndms > 0 && ndms <= kMaxDms, "coherent dedispersion: 1..%d DMs", kMaxDms);
     SW_REQUIRE(d_setup && nchans > 0, "coherent dedispersion: bad setup arguments");
-    const Plan P = make_plan(logn);
+    const int plog = logn > kSplitLog ? kSplitLog : logn;
+    const Plan P = make_plan(plog);
     c32* tw = static_cast<c32*>(d_setup);
     c32* ch = tw + P.tw_total + 16;  // keep the chirp table 128-byte aligned-ish
-    twiddle_k<<<64, 256, 0, as_cuda(stream)>>>(tw, logn);
+    twiddle_k<<<64, 256, 0, as_cuda(stream)>>>(tw, plog);
     SW_LAUNCH_CHECK();
     SetupArgs S{};
     S.logn      = logn;
@@ -596,19 +864,40 @@ int sw_cdd_chirps(const float* h_dms, int ndms, int nchans, int fft_len,
     S.fine_bw   = S.coarse_bw / fft_len;
     for(int d = 0; d < ndms; ++d)
         S.prefactor[d] = -1.0 * (2.0 * 3.1415926535897932385) * 4.148806423e15 * (double)h_dms[d];
-    chirp_k<<<148 * 4, 256, 0, as_cuda(stream)>>>(ch, S);
-    SW_LAUNCH_CHECK();
+    if(logn > kSplitLog) {
+        const int split = fft_len / kSplitM;
+        chirp_split_k<<<148 * 4, 256, 0, as_cuda(stream)>>>(ch, S, split);
+        SW_LAUNCH_CHECK();
+        split_twiddle_k<<<64, 256, 0, as_cuda(stream)>>>(ch + (size_t)ndms * nchans * fft_len,
+                                                         split);
+        SW_LAUNCH_CHECK();
+    } else {
+        chirp_k<<<148 * 4, 256, 0, as_cuda(stream)>>>(ch, S);
+        SW_LAUNCH_CHECK();
+    }
     return SW_OK;
 }
 
-int sw_coherent_dedisperse(const void* d_fpact_in, size_t row_stride,
-                           int nchans, int npol, int nant, int nsamples,
-                           int fft_len, int overlap, const void* d_setup,
-                           int ndms, void* const* h_d_out,
-                           size_t out_row_stride, sw_stream_t stream)
+size_t sw_cdd_workspace_bytes(int nchans, int npol, int nant, int nsamples, int fft_len,
+                              int overlap, int ndms)
 {
     const int logn = log2_exact(fft_len);
-    SW_REQUIRE(logn >= 8 && logn <= 13, "coherent dedispersion: fft_len must be a power of two in [256, 8192]");
+    if(logn <= kSplitLog) return 0;
+    if(logn > 16 || overlap < 0 || overlap >= fft_len || nsamples <= 0 || ndms <= 0) return 0;
+    const size_t items = (size_t)nchans * npol * nant * cdiv(nsamples, fft_len - overlap);
+    return items * ndms * fft_len * sizeof(c32);
+}
+
+int sw_coherent_dedisperse_ws(const void* d_fpact_in, size_t row_stride, int nchans, int npol,
+                              int nant, int nsamples, int fft_len, int overlap,
+                              const void* d_setup, int ndms, void* const* h_d_out,
+                              size_t out_row_stride, void* d_workspace,
+                              size_t workspace_bytes, float* d_debug_f32,
+                              sw_stream_t stream)
+{
+    const int logn = log2_exact(fft_len);
+    SW_REQUIRE(logn >= 8 && logn <= 16,
+               "coherent dedispersion: fft_len must be a power of two in [256, 65536]");
     SW_REQUIRE(d_fpact_in && d_setup && h_d_out, "coherent dedispersion: null pointer");
     SW_REQUIRE(ndms > 0 && ndms <= kMaxDms, "coherent dedispersion: 1..%d DMs", kMaxDms);
     SW_REQUIRE(overlap >= 0 && overlap % 2 == 0 && overlap < fft_len,
@@ -616,24 +905,63 @@ int sw_coherent_dedisperse(const void* d_fpact_in, size_t row_stride,
     SW_REQUIRE(nsamples > 0 && (size_t)overlap + nsamples <= row_stride,
                "coherent dedispersion: input rows must hold history + gulp");
     SW_REQUIRE((size_t)nsamples <= out_row_stride, "coherent dedispersion: output rows too short");
-    const Plan P = make_plan(logn);
+    SW_REQUIRE(nchans > 0 && npol > 0 && nant > 0, "coherent dedispersion: empty shape");
+    const int plog = logn > kSplitLog ? kSplitLog : logn;
+    const Plan P = make_plan(plog);
+    const c32* tw = static_cast<const c32*>(d_setup);
+    const c32* ch = tw + P.tw_total + 16;
+    const int nstreams = nchans * npol * nant;
+    const int nseg = cdiv(nsamples, fft_len - overlap);
+    cudaStream_t s = as_cuda(stream);
+    if(logn > kSplitLog) {
+        const size_t per_item = (size_t)ndms * fft_len * sizeof(c32);
+        SW_REQUIRE(d_workspace && workspace_bytes >= per_item,
+                   "coherent dedispersion: fft_len %d needs a workspace of at least %zu bytes "
+                   "(sw_cdd_workspace_bytes)", fft_len, per_item);
+        SplitArgs a{};
+        a.in = static_cast<const uint8_t*>(d_fpact_in);
+        a.row_stride = row_stride;
+        a.nstreams = nstreams;
+        a.nsamples = nsamples;
+        a.overlap = overlap;
+        a.nseg = nseg;
+        a.ndms = ndms;
+        a.npa = npol * nant;
+        a.tw = tw;
+        a.chirp = ch;
+        a.tws = ch + (size_t)ndms * nchans * fft_len;
+        a.z = static_cast<c32*>(d_workspace);
+        for(int d = 0; d < ndms; ++d) {
+            SW_REQUIRE(h_d_out[d], "coherent dedispersion: null output for DM %d", d);
+            a.out[d] = static_cast<uint8_t*>(h_d_out[d]);
+        }
+        a.out_stride = out_row_stride;
+        a.dbg = reinterpret_cast<float2*>(d_debug_f32);
+        const int items = nstreams * nseg;
+        const size_t ws_items = std::min<size_t>(workspace_bytes / per_item, (size_t)items);
+        switch(fft_len / kSplitM) {
+        case 2: return launch_split<2>(a, items, ws_items, s);
+        case 4: return launch_split<4>(a, items, ws_items, s);
+        default: return launch_split<8>(a, items, ws_items, s);
+        }
+    }
     Args a{};
     a.in         = static_cast<const uint8_t*>(d_fpact_in);
     a.row_stride = row_stride;
     a.npa        = npol * nant;
-    a.nstreams   = nchans * npol * nant;
+    a.nstreams   = nstreams;
     a.nsamples   = nsamples;
     a.overlap    = overlap;
-    a.nseg       = cdiv(nsamples, fft_len - overlap);
+    a.nseg       = nseg;
     a.ndms       = ndms;
-    a.tw         = static_cast<const c32*>(d_setup);
-    a.chirp      = a.tw + P.tw_total + 16;
+    a.tw         = tw;
+    a.chirp      = ch;
     for(int d = 0; d < ndms; ++d) {
         SW_REQUIRE(h_d_out[d], "coherent dedispersion: null output for DM %d", d);
         a.out[d] = static_cast<uint8_t*>(h_d_out[d]);
     }
     a.out_stride = out_row_stride;
-    cudaStream_t s = as_cuda(stream);
+    a.dbg        = reinterpret_cast<float2*>(d_debug_f32);
     switch(logn) {
     case 8: return launch_logn<8>(a, s);
     case 9: return launch_logn<9>(a, s);
@@ -642,6 +970,20 @@ int sw_coherent_dedisperse(const void* d_fpact_in, size_t row_stride,
     case 12: return launch_logn<12>(a, s);
     default: return launch_logn<13>(a, s);
     }
+}
+
+int sw_coherent_dedisperse(const void* d_fpact_in, size_t row_stride,
+                           int nchans, int npol, int nant, int nsamples,
+                           int fft_len, int overlap, const void* d_setup,
+                           int ndms, void* const* h_d_out,
+                           size_t out_row_stride, sw_stream_t stream)
+{
+    SW_REQUIRE(fft_len <= kSplitM,
+               "coherent dedispersion: fft_len %d > %d needs sw_coherent_dedisperse_ws", fft_len,
+               kSplitM);
+    return sw_coherent_dedisperse_ws(d_fpact_in, row_stride, nchans, npol, nant, nsamples,
+                                     fft_len, overlap, d_setup, ndms, h_d_out, out_row_stride,
+                                     nullptr, 0, nullptr, stream);
 }
 
 }  // extern "C"

@@ -189,8 +189,13 @@ class CoherentDedisperser:
         call("sw_cdd_chirps", dms_c, len(dms), nchans, fft_len, ctypes.c_double(low_freq),
              ctypes.c_double(bw), _ptr(self.setup), _stream())
 
-    def dedisperse(self, fpact_ext, nsamples, outs=None, stream=None):
-        """fpact_ext rows hold `overlap` history samples then the gulp."""
+    def dedisperse(self, fpact_ext, nsamples, outs=None, stream=None, debug=False,
+                   workspace_limit=2 << 30):
+        """fpact_ext rows hold `overlap` history samples then the gulp.
+        fft_len > 8192 runs the split transform through a device workspace of
+        at most `workspace_limit` bytes (segments are processed in chunks).
+        debug=True also returns the float dedispersed voltages before
+        rounding, [ndms][F][P][A][nsamples][re|im]."""
         F, P, A, _, stride = fpact_ext.shape
         if F != self.nchans:
             raise ValueError(f"voltages have {F} channels but the chirp tables {self.nchans}")
@@ -199,10 +204,18 @@ class CoherentDedisperser:
             outs = [torch.empty((F, P, A, 2, nsamples), dtype=torch.int8,
                                 device=fpact_ext.device) for _ in range(nd)]
         arr = (ctypes.c_void_p * nd)(*[o.data_ptr() for o in outs])
-        call("sw_coherent_dedisperse", _ptr(fpact_ext), stride, F, P, A, nsamples,
+        need = lib().sw_cdd_workspace_bytes(F, P, A, nsamples, self.fft_len, self.overlap, nd)
+        ws = None
+        if need:
+            per_seg = nd * self.fft_len * 8
+            nbytes = max(per_seg, min(need, workspace_limit) // per_seg * per_seg)
+            ws = torch.empty(nbytes, dtype=torch.uint8, device=fpact_ext.device)
+        dbg = (torch.empty((nd, F, P, A, nsamples, 2), dtype=torch.float32,
+                           device=fpact_ext.device) if debug else None)
+        call("sw_coherent_dedisperse_ws", _ptr(fpact_ext), stride, F, P, A, nsamples,
              self.fft_len, self.overlap, _ptr(self.setup), nd, arr, outs[0].shape[-1],
-             _stream(stream))
-        return outs
+             _ptr(ws), ws.numel() if ws is not None else 0, _ptr(dbg), _stream(stream))
+        return (outs, dbg) if debug else outs
 
 
 # ----------------------------------------------------- incoherent dedisp.

@@ -171,3 +171,52 @@ def test_pipeline_full_stokes_iquv(cuda, oracle):
     assert np.array_equal(out["ib_raw"], raw_ref)
     assert np.array_equal(out["ib"], ib_ref)
     assert np.array_equal(out["cb"], cb_ref)
+
+
+def test_dispersed_pulse_peaks_in_its_dm_fft65536(cuda, oracle):
+    """Coherent dedispersion with 2^16-point FFTs in the pipeline: a burst
+    dispersed within each channel at DM 150 (by the conjugate of the DM 150
+    response, i.e. what the sky does) and arriving at boresight must come out
+    strongest in the DM 150 coherent beam, and be re-compressed there."""
+    torch = cuda
+    from skyweaver_b200 import stages, synthetic
+    g = synthetic.rng(150)
+    A, F, B, T, ts, N = 16, 4, 32, 65536, 16, 65536
+    dms = [0.0, 50.0, 150.0, 500.0]
+    chbw = 856e6 / 1024
+    bw = F * chbw
+    centre = 1284e6 - 30 * chbw                  # bottom of the L-band subband
+    low = float(np.float32(centre - bw / 2))
+    # noise + a 32-sample burst at t0, dispersed per channel at DM 150
+    v = g.normal(0, 8, size=(F, T, 2, A, 2))
+    t0, W, amp = 30000, 32, 4.0
+    H = oracle.chirp(F, N, low, bw, 150.0)       # DM 150 dedispersion response
+    for c in range(F):
+        burst = np.zeros(N, np.complex128)
+        burst[t0 % N: t0 % N + W] = amp
+        disp = np.fft.ifft(np.fft.fft(burst) * np.conj(H[c]))
+        v[c, :N, :, :, 0] += disp.real[:, None, None]
+        v[c, :N, :, :, 1] += disp.imag[:, None, None]
+    ftpa = np.clip(np.rint(v), -127, 127).astype(np.int8)          # [F][T][P][A][2]
+    taftp = ftpa.reshape(F, T // 256, 256, 2, A, 2).transpose(1, 4, 0, 2, 3, 5).copy()
+    delays = synthetic.delay_model(g, B, A)
+    delays[0] = [1.0, 0.0, 0.0]                  # beam 0 at boresight
+    mapping = np.zeros(B, np.int32)
+    pipe = stages.BeamformerPipeline(nantennas=A, input_nantennas=A, nchans=F, nbeams=B,
+                                     gulp_samples=T, tscrunch=ts, centre_frequency=centre,
+                                     bandwidth=bw, dms=dms, beamset_weights=np.ones((1, A)),
+                                     beamset_mapping=mapping, fft_len=N)
+    assert pipe.fft_plan()[0] == N
+    pipe.set_delays(delays, 1.7e9)
+    pipe.process_device(torch.from_numpy(taftp).cuda(), 1.7e9)
+    series = []
+    for d in range(len(dms)):
+        cb = pipe.outputs(d)["cb"][:, :, 0].astype(np.float64).sum(axis=1)   # [T/ts]
+        series.append(np.convolve(cb, np.ones(2), "valid"))                 # 2-bin boxcar
+    pipe.close()
+    peaks = [s.max() for s in series]
+    print("boxcar peak per DM:", dict(zip(dms, peaks)))
+    assert int(np.argmax(peaks)) == dms.index(150.0), peaks
+    # re-compressed: the DM 150 peak stands well above its own noise
+    s = series[2]
+    assert (s.max() - np.median(s)) > 6 * s.std()

@@ -279,7 +279,8 @@ def test_coherent_dedispersion_golden_vector(cuda):
 
 
 @pytest.mark.parametrize("fft_len,dms", [(2048, [0.0, 50.0, 150.0]), (4096, [0.0, 500.0]),
-                                         (8192, [150.0]), (1024, [30.0])])
+                                         (8192, [150.0]), (1024, [30.0]),
+                                         (16384, [0.0, 500.0]), (32768, [150.0])])
 def test_coherent_dedispersion_overlap_save(cuda, oracle, fft_len, dms):
     from skyweaver_b200 import stages, synthetic
     g = synthetic.rng(fft_len)
@@ -303,6 +304,42 @@ def test_coherent_dedispersion_overlap_save(cuda, oracle, fft_len, dms):
         frac = (diff > 0).mean()
         assert diff.max() <= 1, (dm, diff.max())
         assert frac < 1e-3, (dm, frac)
+
+
+def test_coherent_dedispersion_fft65536_precision(cuda, oracle):
+    """Precision study with 2^16-point overlap-save FFTs (L-band, 64-channel
+    subband bottom, DMs {0, 50, 150, 500}): the float dedispersed voltages
+    before requantisation against the FP64 oracle, and the int8 outputs
+    within one LSB.  The workspace is limited so that the segments run in
+    several chunks."""
+    from skyweaver_b200 import stages, synthetic
+    g = synthetic.rng(65536)
+    F, A, T, N = 2, 4, 98304, 65536
+    dms = [0.0, 50.0, 150.0, 500.0]
+    chbw = 856e6 / 1024
+    bw = F * chbw
+    low = 1284e6 - 32 * chbw
+    smear = stages.dm_delay(low, low + chbw, max(dms)) * chbw
+    overlap = int(math.ceil(smear)) + 15 & ~15
+    ext = np.clip(np.rint(g.normal(0, 8, size=(F, 2, A, 2, overlap + T))), -127, 127).astype(np.int8)
+    cdd = stages.CoherentDedisperser(F, A, N, overlap, low, bw, dms)
+    outs, dbg = cdd.dedisperse(_dev(cuda, ext), T, debug=True,
+                               workspace_limit=3 * len(dms) * N * 8)
+    dbg = _np(dbg)                                   # [D][F][P][A][T][2]
+    ftpa_ext = ext.transpose(0, 4, 1, 2, 3)
+    for d, dm in enumerate(dms):
+        ref, f64 = oracle.cdd_ftpa(ftpa_ext, T, oracle.chirp(F, N, low, bw, dm), overlap,
+                                   want_f64=True)
+        got_f = dbg[d][..., 0] + 1j * dbg[d][..., 1]  # [F][P][A][T]
+        want_f = f64.transpose(0, 2, 3, 1)
+        err = np.abs(got_f - want_f)
+        rms_rel = math.sqrt(np.mean(err ** 2) / np.mean(np.abs(want_f) ** 2))
+        print(f"DM {dm}: max |err| {err.max():.3e}, rms rel {rms_rel:.3e}")
+        assert rms_rel < 1e-5, (dm, rms_rel)
+        assert err.max() < 0.05, (dm, err.max())
+        got = _np(outs[d]).transpose(0, 4, 1, 2, 3)
+        diff = np.abs(got.astype(int) - ref.astype(int))
+        assert diff.max() <= 1 and (diff > 0).mean() < 1e-3, (dm, (diff > 0).mean())
 
 
 # ------------------------------------------------- incoherent dedispersion
