@@ -285,6 +285,43 @@ int sw_incoherent_dedisperse(const int8_t* d_tfb, int nsamples, int nchans,
                              int8_t* d_tdb, sw_stream_t stream);
 
 /* ------------------------------------------------------------------ */
+/* IncoherentDedispersionPipeline (device-resident AggregationBuffer)   */
+/* ------------------------------------------------------------------ */
+/* Replaces IncoherentDedispersionPipeline<In,Out,Handler>
+ * (cpp/skyweaver/IncoherentDedispersionPipeline.cuh,
+ *  cpp/skyweaver/detail/IncoherentDedispersionPipeline.cu:6-113) and its
+ * AggregationBuffer (cpp/skyweaver/detail/AggregationBuffer.cu:23-117) with
+ * the buffer in device memory. One block per coherent DM of the
+ * DedispersionPlan; each block aggregates int8 TFB [T][nchans][nbeams]
+ * (nbeams counts Stokes components: 4 x beams for IQUV), and every
+ * `dispatch` new samples (after the first dispatch + overlap) runs the
+ * incoherent dedisperser on the buffer and calls the handler with the TDB
+ * result [dispatch / tscrunch][ndms][nbeams] in device memory, on the
+ * pushing stream, before the buffer's overlap moves to its front. */
+typedef struct sw_idd_pipeline sw_idd_pipeline;
+typedef void (*sw_idd_handler)(void* user, int block, const int8_t* d_tdb,
+                               int nsamples_out, int ndms, int nbeams,
+                               sw_stream_t stream);
+
+/* h_delays[b]: int [h_ndms[b]][nchans] sample delays of block b (the
+ * IncoherentDedisperser's delays(), overlap = their maximum); h_scale[b] its
+ * scale factor; h_dispatch may be NULL for the reference's default
+ * max(10 x max delay, 8192) rounded down to a multiple of tscrunch. */
+int sw_idd_pipeline_create(int nchans, int nbeams, int nblocks,
+                           const int* h_ndms, const int* const* h_delays,
+                           const int* h_tscrunch, const float* h_scale,
+                           const int* h_dispatch, sw_idd_handler handler,
+                           void* user, sw_idd_pipeline** out);
+void sw_idd_pipeline_destroy(sw_idd_pipeline* p);
+/* AggregationBuffer::push_back for block `block` (operator()(data, dm_idx)):
+ * nsamples time samples of device TFB. */
+int sw_idd_pipeline_push(sw_idd_pipeline* p, int block, const int8_t* d_tfb,
+                         size_t nsamples, sw_stream_t stream);
+int sw_idd_pipeline_geometry(const sw_idd_pipeline* p, int block,
+                             int* dispatch_size, int* overlap,
+                             int* nsamples_out, int* ndms);
+
+/* ------------------------------------------------------------------ */
 /* BeamformerPipeline                                                   */
 /* ------------------------------------------------------------------ */
 /* Replaces BeamformerPipeline<CBH,IBH,StatsH,BfTraits>

@@ -17,6 +17,7 @@
 #include <cstdint>
 #include <cstring>
 #include <fstream>
+#include <memory>
 #include <sstream>
 #include <stdexcept>
 #include <string>
@@ -520,6 +521,7 @@ class IncoherentDedisperser {
     }
     const std::vector<int>& delays() const { return _delays; }
     int max_sample_delay() const { return _max; }
+    float scale_factor() const { return _scale; }
     // int8 TFB [T][F][B] -> int8 TDB [(T - max_delay)/tscrunch][ndms][B]
     void dedisperse(const DeviceBuffer<int8_t>& tfb, DeviceBuffer<int8_t>& tdb, cudaStream_t stream = 0)
     {
@@ -560,6 +562,62 @@ class IncoherentDedisperser {
     float _scale = 1.0f;
 };
 
+// ------------------------------------------- IncoherentDedispersionPipeline
+// IncoherentDedispersionPipeline<In, Out, Handler>
+// (detail/IncoherentDedispersionPipeline.cu:6-113) with the AggregationBuffer
+// in device memory.  One block per DedispersionPlan block (coherent DM); the
+// handler is called as handler(d_tdb, nsamples_out, ndms, nbeams, ref_dm_idx)
+// with the TDB result in device memory, ordered on the pushing stream.
+template <typename Handler>
+class IncoherentDedispersionPipeline {
+  public:
+    IncoherentDedispersionPipeline(const PipelineConfig& config, const DedispersionPlan& plan,
+                                   Handler& handler)
+        : _config(config), _handler(handler)
+    {
+        const auto& blocks = plan.blocks();
+        const int ncomp = (int)config.stokes_components();
+        std::vector<int> ndms, ts;
+        std::vector<float> scale;
+        std::vector<const int*> dptr;
+        for(const auto& b : blocks) {
+            _dedispersers.emplace_back(new IncoherentDedisperser(config, b.incoherent_dms,
+                                                                 (std::size_t)b.tscrunch));
+            ndms.push_back((int)b.incoherent_dms.size());
+            ts.push_back(b.tscrunch);
+            scale.push_back(_dedispersers.back()->scale_factor());
+        }
+        for(auto& d : _dedispersers) dptr.push_back(d->delays().data());
+        check(sw_idd_pipeline_create((int)config.nchans(), (int)config.nbeams() * ncomp,
+                                     (int)blocks.size(), ndms.data(), dptr.data(), ts.data(),
+                                     scale.data(), nullptr, &trampoline, this, &_p));
+    }
+    ~IncoherentDedispersionPipeline() { sw_idd_pipeline_destroy(_p); }
+    IncoherentDedispersionPipeline(const IncoherentDedispersionPipeline&) = delete;
+    IncoherentDedispersionPipeline& operator=(const IncoherentDedispersionPipeline&) = delete;
+
+    // operator()(data, ref_dm_idx): push nsamples of device TFB
+    void operator()(const int8_t* d_tfb, std::size_t nsamples, std::size_t ref_dm_idx,
+                    cudaStream_t stream = 0)
+    {
+        check(sw_idd_pipeline_push(_p, (int)ref_dm_idx, d_tfb, nsamples, (sw_stream_t)stream));
+    }
+    const IncoherentDedisperser& dedisperser(std::size_t i) const { return *_dedispersers[i]; }
+
+  private:
+    static void trampoline(void* user, int block, const int8_t* d_tdb, int nout, int ndms,
+                           int nbeams, sw_stream_t)
+    {
+        auto* self = static_cast<IncoherentDedispersionPipeline*>(user);
+        self->_handler(d_tdb, (std::size_t)nout, (std::size_t)ndms, (std::size_t)nbeams,
+                       (std::size_t)block);
+    }
+    const PipelineConfig& _config;
+    Handler& _handler;
+    std::vector<std::unique_ptr<IncoherentDedisperser>> _dedispersers;
+    sw_idd_pipeline* _p = nullptr;
+};
+
 // -------------------------------------------------------- BeamformerPipeline
 // cpp/skyweaver/BeamformerPipeline.cuh:48-67.  Handlers get host copies:
 // cb_handler(const int8_t* tfb, std::size_t bytes, std::size_t dm_idx).
@@ -594,6 +652,25 @@ class BeamformerPipeline {
         _out.resize(sw_pipeline_cb_bytes_per_dm(_p) * c.ndms);
     }
     ~BeamformerPipeline() { sw_pipeline_destroy(_p); }
+    // one gulp of TAFTP voltages already in device memory; each DM's
+    // coherent beams stay on the device and go to
+    // handler(d_tfb, nsamples, dm_idx, stream), ordered on `stream` (the
+    // call signature of IncoherentDedispersionPipeline, which makes the
+    // reference's CB handler -> incoherent dedispersion chain device-resident)
+    template <typename DeviceHandler>
+    void process_device(const void* d_taftp, double epoch, DeviceHandler& handler,
+                        cudaStream_t stream = 0)
+    {
+        const auto& d = _delays.delays(epoch);
+        check(sw_pipeline_set_delays(_p, d.download().data(), _delays.epoch()));
+        check(sw_pipeline_process_device(_p, d_taftp, epoch, (sw_stream_t)stream));
+        const std::size_t nsamp = _config.gulp_length_samps() / _config.cb_tscrunch();
+        for(std::size_t dm = 0; dm < _config.coherent_dms().size(); ++dm) {
+            const int8_t* cb = nullptr;
+            check(sw_pipeline_outputs(_p, (int)dm, &cb, nullptr, nullptr, nullptr));
+            handler(cb, nsamp, dm, stream);
+        }
+    }
     // one gulp of pinned TAFTP voltages; epoch = UNIX time of the gulp start
     void operator()(const void* h_taftp, double epoch)
     {

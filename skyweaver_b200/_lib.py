@@ -16,6 +16,7 @@ c_void_p = ctypes.c_void_p
 c_float_p = ctypes.POINTER(ctypes.c_float)
 
 SW_OK = 0
+IDD_HANDLER = ctypes.CFUNCTYPE(None, c_void_p, c_int, c_void_p, c_int, c_int, c_int, c_void_p)
 STOKES = {"I": 0, "Q": 1, "U": 2, "V": 3, "IQUV": 4}
 
 
@@ -94,6 +95,15 @@ _SIGS = {
     "sw_coherent_dedisperse_ws": (c_int, [c_void_p, c_size_t, c_int, c_int, c_int, c_int, c_int,
                                           c_int, c_void_p, c_int, ctypes.POINTER(c_void_p),
                                           c_size_t, c_void_p, c_size_t, c_void_p, c_void_p]),
+    "sw_idd_pipeline_create": (c_int, [c_int, c_int, c_int, ctypes.POINTER(c_int),
+                                       ctypes.POINTER(c_void_p), ctypes.POINTER(c_int),
+                                       c_float_p, ctypes.POINTER(c_int), c_void_p, c_void_p,
+                                       ctypes.POINTER(c_void_p)]),
+    "sw_idd_pipeline_destroy": (None, [c_void_p]),
+    "sw_idd_pipeline_push": (c_int, [c_void_p, c_int, c_void_p, c_size_t, c_void_p]),
+    "sw_idd_pipeline_geometry": (c_int, [c_void_p, c_int, ctypes.POINTER(c_int),
+                                         ctypes.POINTER(c_int), ctypes.POINTER(c_int),
+                                         ctypes.POINTER(c_int)]),
     "sw_incoherent_dedisperse": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_int,
                                          c_int, c_int, c_float, c_void_p, c_void_p]),
     "sw_pipeline_create": (c_int, [ctypes.POINTER(PipelineConfig), ctypes.POINTER(c_void_p)]),

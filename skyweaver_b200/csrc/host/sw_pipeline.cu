@@ -53,12 +53,6 @@ struct DevBuf {
     T* as() const { return static_cast<T*>(p); }
 };
 
-#define SW_TRY(expr)                 \
-    do {                             \
-        int _rc = (expr);            \
-        if(_rc != SW_OK) return _rc; \
-    } while(0)
-
 }  // namespace
 
 struct sw_pipeline {

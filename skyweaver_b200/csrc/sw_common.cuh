@@ -50,6 +50,13 @@ inline cudaStream_t as_cuda(sw_stream_t s) { return reinterpret_cast<cudaStream_
 
 #define SW_LAUNCH_CHECK() SW_CUDA_CHECK(cudaGetLastError())
 
+// Propagate a non-OK SW status.
+#define SW_TRY(expr)                 \
+    do {                             \
+        int _rc = (expr);            \
+        if(_rc != SW_OK) return _rc; \
+    } while(0)
+
 namespace swb {
 
 // ceil division

@@ -235,6 +235,49 @@ def incoherent_dedisperse(tfb, delays, max_delay, tscrunch, scale_factor, stream
     return out
 
 
+class IncoherentDedispersionPipeline:
+    """IncoherentDedispersionPipeline (detail/IncoherentDedispersionPipeline.cu:
+    6-113) with its AggregationBuffer (detail/AggregationBuffer.cu:23-117) in
+    device memory.  blocks: one (delays int [ndms][F], tscrunch, scale_factor)
+    per coherent DM.  push(block, tfb) appends int8 TFB [T][F][nbeams]
+    (nbeams counting Stokes components); each dispatch calls
+    handler(block, tdb) with a device copy of the TDB
+    [dispatch / tscrunch][ndms][nbeams]."""
+
+    def __init__(self, nchans, nbeams, blocks, handler, dispatch=None):
+        self.handler = handler
+        nb = len(blocks)
+        self._delays = [np.ascontiguousarray(b[0], np.int32) for b in blocks]
+        ndms = (ctypes.c_int * nb)(*[d.shape[0] for d in self._delays])
+        dptr = (ctypes.c_void_p * nb)(*[d.ctypes.data for d in self._delays])
+        ts = (ctypes.c_int * nb)(*[int(b[1]) for b in blocks])
+        sc = (ctypes.c_float * nb)(*[float(b[2]) for b in blocks])
+        disp = (ctypes.c_int * nb)(*dispatch) if dispatch is not None else None
+        self._cb = _lib.IDD_HANDLER(self._on_dispatch)
+        h = ctypes.c_void_p()
+        call("sw_idd_pipeline_create", nchans, nbeams, nb, ndms, dptr, ts, sc, disp,
+             ctypes.cast(self._cb, ctypes.c_void_p), None, ctypes.byref(h))
+        self.h = h
+
+    def _on_dispatch(self, user, block, ptr, nout, ndms, nbeams, stream):
+        # runs on the pushing thread, ordered on the pushing stream
+        tdb = _device_view(ptr, nout * ndms * nbeams).clone().view(torch.int8)
+        self.handler(block, tdb.reshape(nout, ndms, nbeams))
+
+    def push(self, block, tfb, stream=None):
+        call("sw_idd_pipeline_push", self.h, block, _ptr(tfb), tfb.shape[0], _stream(stream))
+
+    def geometry(self, block):
+        v = [ctypes.c_int() for _ in range(4)]
+        call("sw_idd_pipeline_geometry", self.h, block, *[ctypes.byref(x) for x in v])
+        return tuple(x.value for x in v)  # dispatch, overlap, nsamples_out, ndms
+
+    def close(self):
+        if self.h:
+            lib().sw_idd_pipeline_destroy(self.h)
+            self.h = None
+
+
 # ------------------------------------------------------------------ pipeline
 class BeamformerPipeline:
     """sw_pipeline_*: the graph-captured per-gulp chain (BeamformerPipeline)."""

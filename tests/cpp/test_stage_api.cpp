@@ -255,6 +255,65 @@ static void pipeline_smoke(const std::string& golden)
     std::puts("PASS beamformer_pipeline");
 }
 
+struct TdbCollector {
+    std::vector<std::vector<int8_t>> got[2];
+    std::size_t nbeams = 0, ndms[2] = {0, 0};
+    void operator()(const int8_t* d_tdb, std::size_t nout, std::size_t ndm, std::size_t nb,
+                    std::size_t block)
+    {
+        std::vector<int8_t> h(nout * ndm * nb);
+        cuda_check(cudaMemcpy(h.data(), d_tdb, h.size(), cudaMemcpyDeviceToHost), "tdb");
+        got[block].push_back(std::move(h));
+        nbeams = nb;
+        ndms[block] = ndm;
+    }
+};
+
+// IncoherentDedispersionPipeline.cu:6-113 + AggregationBuffer.cu:23-117:
+// all-ones TFB gives sqrt(nchans * tscrunch) (truncated) in every output, and
+// block b dispatches floor((T - overlap) / dispatch) times
+static void idd_pipeline_tests()
+{
+    PipelineConfig c = base_config();
+    c.nchans(64);
+    c.nbeams(32);
+    c.bandwidth(32e6);
+    c.centre_frequency(580e6);
+    c.cb_tscrunch(16);
+    DedispersionPlan plan;
+    plan.add_block("5.0:0.0:20.0:5.0:1");
+    plan.add_block("30.0:25.0:45.0:10.0:2");
+    TdbCollector col;
+    IncoherentDedispersionPipeline<TdbCollector> idd(c, plan, col);
+    const std::size_t T = 40000, slot = c.nchans() * c.nbeams();
+    DeviceBuffer<int8_t> ones;
+    ones.upload(std::vector<int8_t>(T * slot, 1));
+    for(int b = 0; b < 2; ++b) {
+        std::size_t pos = 0;
+        for(std::size_t n : {1000u, 17u, 20000u, 18983u}) {
+            idd(ones.data() + pos * slot, n, b);
+            pos += n;
+        }
+        EXPECT(pos == T);
+    }
+    cuda_check(cudaDeviceSynchronize(), "idd pipeline");
+    for(int b = 0; b < 2; ++b) {
+        const auto& d = idd.dedisperser(b);
+        const std::size_t O = d.max_sample_delay();
+        std::size_t D = std::max<std::size_t>(O * 10, 8192);
+        const std::size_t ts = plan[b].tscrunch;
+        D -= D % ts;
+        EXPECT(col.got[b].size() == (T - O) / D);
+        EXPECT(col.ndms[b] == plan[b].incoherent_dms.size());
+        const int8_t want = (int8_t)std::sqrt((double)(c.nchans() * ts));
+        for(const auto& v : col.got[b]) {
+            EXPECT(v.size() == D / ts * col.ndms[b] * c.nbeams());
+            for(int8_t x : v) EXPECT(x == want);
+        }
+    }
+    std::puts("PASS incoherent_dedispersion_pipeline");
+}
+
 int main(int argc, char** argv)
 {
     const std::string golden = argc > 1 ? argv[1] : "tests/golden";
@@ -266,6 +325,7 @@ int main(int argc, char** argv)
     delay_manager_tests(golden);
     dedispersion_plan_tests();
     pipeline_smoke(golden);
+    idd_pipeline_tests();
     std::puts("ALL PASS");
     return 0;
 }

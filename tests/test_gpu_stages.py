@@ -393,3 +393,42 @@ def test_incoherent_dedispersion_char4_iquv(cuda, oracle):
     for c in range(4):
         ref = oracle.idd(np.ascontiguousarray(tfb[..., c]), delays, maxd, ts, sf)
         assert np.array_equal(got[..., c], ref)
+
+
+def test_incoherent_dedispersion_pipeline_aggregation(cuda, oracle):
+    """Device AggregationBuffer semantics (AggregationBuffer.cu:23-117): with
+    dispatch D and overlap O = max delay, dispatch k covers samples
+    [k D, (k+1) D + O) of the pushed stream, whatever the push sizes."""
+    from skyweaver_b200 import stages, synthetic
+    g = synthetic.rng(43)
+    F, B = 16, 8
+    freqs = synthetic.channel_frequencies(1284e6, F * 856e6 / 1024, F)
+    tsamp = 16 / (856e6 / 1024)
+    blocks, refs = [], []
+    for dms, ts in (([0.0, 40.0, 80.0], 2), ([250.0, 300.0], 4)):
+        delays, maxd = oracle.idd_delays(freqs, np.array(dms, np.float32), tsamp)
+        sf = np.float32(math.sqrt(F * ts))
+        blocks.append((delays, ts, float(sf)))
+        refs.append((delays, maxd, ts, sf))
+    got = {0: [], 1: []}
+    pipe = stages.IncoherentDedispersionPipeline(F, B, blocks, lambda b, t: got[b].append(t),
+                                                 dispatch=[512, 1000])
+    total = 6000
+    stream = g.integers(-128, 128, size=(total, F, B), dtype=np.int8)
+    for blk in (0, 1):
+        pos = 0
+        for n in (1, 700, 33, 2048, 1500, 1718):
+            pipe.push(blk, _dev(cuda, stream[pos:pos + n]))
+            pos += n
+        assert pos == total
+    geo = [pipe.geometry(b) for b in (0, 1)]
+    pipe.close()
+    for blk, (delays, maxd, ts, sf) in enumerate(refs):
+        D, O, nout, nd = geo[blk]
+        assert O == maxd and nout == D // ts
+        nk = (total - O) // D
+        assert len(got[blk]) == nk
+        for k in range(nk):
+            ref = oracle.idd(np.ascontiguousarray(stream[k * D:(k + 1) * D + O]), delays, maxd,
+                             ts, sf)
+            assert np.array_equal(_np(got[blk][k]), ref), (blk, k)
