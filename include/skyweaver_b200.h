@@ -198,6 +198,7 @@ typedef struct sw_cb_shape {
     int ib_subtract;    /* SKYWEAVER_IB_SUBTRACTION (default 1)           */
     size_t row_stride;  /* FPACT row stride (samples)                     */
     size_t sample_offset;
+    int tiles_per_item; /* 64-sample tiles per work item (0: 16; see sw_autotune) */
 } sw_cb_shape;
 
 /* Replaces CoherentBeamformer<BfTraits>::beamform
@@ -322,6 +323,28 @@ int sw_idd_pipeline_geometry(const sw_idd_pipeline* p, int block,
                              int* nsamples_out, int* ndms);
 
 /* ------------------------------------------------------------------ */
+/* Autotuner                                                            */
+/* ------------------------------------------------------------------ */
+/* Times the coherent dedisperser at every FFT length the DM smear allows
+ * and the coherent beamformer at several work-item sizes, on synthetic data
+ * of this exact shape, and returns the fastest choice (cached per key
+ * (nantennas, nbeams, nchans, nsamples, tscrunch, ndms, overlap) for the
+ * process). The reference's launch shapes are compile-time constants
+ * (skyweaver_constants.hpp:28-135); this has no counterpart there. Needs a
+ * few GB of device memory while it runs. */
+typedef struct sw_tuning {
+    int fft_len;            /* coherent dedispersion FFT length          */
+    int overlap;            /* overlap-save overlap (samples)            */
+    int cb_tiles_per_item;  /* sw_cb_shape.tiles_per_item                */
+    float cdd_ms, cb_ms;    /* measured per gulp at the chosen settings  */
+} sw_tuning;
+
+int sw_autotune(int nantennas, int nbeams, int nchans, int nsamples,
+                int tscrunch, int ndms, const float* h_dms,
+                double centre_frequency, double bandwidth, sw_tuning* out,
+                sw_stream_t stream);
+
+/* ------------------------------------------------------------------ */
 /* BeamformerPipeline                                                   */
 /* ------------------------------------------------------------------ */
 /* Replaces BeamformerPipeline<CBH,IBH,StatsH,BfTraits>
@@ -351,6 +374,8 @@ typedef struct sw_pipeline_config {
     int nbeamsets;
     const float* beamset_weights; /* host [nbeamsets][nantennas]         */
     const int* beamset_mapping;   /* host [nbeams]                       */
+    int autotune;           /* 1 = sw_autotune picks fft_len (if 0) and the
+                               beamformer work-item size                 */
 } sw_pipeline_config;
 
 int sw_pipeline_create(const sw_pipeline_config* cfg, sw_pipeline** out);

@@ -198,6 +198,14 @@ class PipelineConfig {
     double _cfreq = 1284000000.0, _bw = 13375000.0;
     float _level = 24.0f;
     std::string _stokes = "I", _delay_file;
+    bool _autotune = false;
+
+  public:
+    // let sw_autotune pick the FFT length and beamformer work-item size
+    bool autotune() const { return _autotune; }
+    void autotune(bool on) { _autotune = on; }
+
+  private:
     DedispersionPlan _plan;
     mutable bool _stale = true;
     mutable std::vector<double> _freqs;
@@ -648,6 +656,7 @@ class BeamformerPipeline {
         c.nbeamsets       = _delays.nbeamsets();
         c.beamset_weights = _delays.beamset_weights().data();
         c.beamset_mapping = _delays.beamset_mapping().data();
+        c.autotune        = config.autotune() ? 1 : 0;
         check(sw_pipeline_create(&c, &_p));
         _out.resize(sw_pipeline_cb_bytes_per_dm(_p) * c.ndms);
     }

@@ -38,7 +38,7 @@ class CbShape(ctypes.Structure):
     _fields_ = [("nchans", c_int), ("nsamples", c_int), ("nantennas", c_int),
                 ("nbeams", c_int), ("tscrunch", c_int), ("stokes", c_int),
                 ("ib_subtract", c_int), ("row_stride", c_size_t),
-                ("sample_offset", c_size_t)]
+                ("sample_offset", c_size_t), ("tiles_per_item", c_int)]
 
 
 class PipelineConfig(ctypes.Structure):
@@ -49,7 +49,13 @@ class PipelineConfig(ctypes.Structure):
                 ("ndms", c_int), ("dms", c_float_p), ("fft_len", c_int),
                 ("enable_coherent_dedispersion", c_int), ("grouped", c_int),
                 ("use_graph", c_int), ("nbeamsets", c_int),
-                ("beamset_weights", c_float_p), ("beamset_mapping", ctypes.POINTER(c_int))]
+                ("beamset_weights", c_float_p), ("beamset_mapping", ctypes.POINTER(c_int)),
+                ("autotune", c_int)]
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [("fft_len", c_int), ("overlap", c_int), ("cb_tiles_per_item", c_int),
+                ("cdd_ms", c_float), ("cb_ms", c_float)]
 
 
 _SIGS = {
@@ -104,6 +110,8 @@ _SIGS = {
     "sw_idd_pipeline_geometry": (c_int, [c_void_p, c_int, ctypes.POINTER(c_int),
                                          ctypes.POINTER(c_int), ctypes.POINTER(c_int),
                                          ctypes.POINTER(c_int)]),
+    "sw_autotune": (c_int, [c_int, c_int, c_int, c_int, c_int, c_int, c_float_p, c_double,
+                            c_double, ctypes.POINTER(Tuning), c_void_p]),
     "sw_incoherent_dedisperse": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_int,
                                          c_int, c_int, c_float, c_void_p, c_void_p]),
     "sw_pipeline_create": (c_int, [ctypes.POINTER(PipelineConfig), ctypes.POINTER(c_void_p)]),

@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "../sw_common.cuh"
+#include "sw_host.hpp"
 
 namespace swb {
 int launch_weights(const float* d_delays, const double* d_freqs, int nant, int nbeams,
@@ -29,7 +30,6 @@ int launch_weights(const float* d_delays, const double* d_freqs, int nant, int n
 
 namespace {
 
-constexpr double kDmConst = 4.148806423e15;  // dedispersion_utils.cuh:12-13
 
 struct DevBuf {
     void* p = nullptr;
@@ -63,6 +63,7 @@ struct sw_pipeline {
     std::vector<double> freqs;
     int nheaps = 0, T = 0, F = 0, A = 0, B = 0, S = 0, ndm = 0, ts = 0;
     int fft_len = 0, overlap = 0;  // overlap: multiple of 16
+    int cb_tpi = 0;                // CB work-item size (0: kernel default)
     size_t ext_stride = 0, ext_off = 0, dd_stride = 0;
     size_t nrows = 0;  // F * P * A * 2
 
@@ -136,23 +137,17 @@ int sw_pipeline::init(const sw_pipeline_config& c)
     // Coherent dedispersion plan: overlap = largest intra-channel DM smear
     // (lowest channel, largest DM), rounded up to a multiple of 16.
     if(c.enable_coherent_dedispersion) {
-        const float f_low = (float)(c.centre_frequency - c.bandwidth / 2.0f);
-        const double tsamp = 1.0 / chbw;
-        double maxdm = 0.0;
-        for(float d : dms) maxdm = std::max(maxdm, (double)d);
-        const double f1 = f_low, f2 = f_low + chbw;
-        const double smear = kDmConst * (1.0 / (f1 * f1) - 1.0 / (f2 * f2)) * maxdm;
-        int ov = (int)std::ceil(smear / tsamp);
-        overlap = (ov + 15) / 16 * 16;
+        overlap = swb::cdd_overlap(c.centre_frequency, c.bandwidth, F, dms.data(), ndm);
         if(c.fft_len > 0) {
             fft_len = c.fft_len;
+        } else if(c.autotune) {
+            sw_tuning tu{};
+            SW_TRY(sw_autotune(A, B, F, T, ts, ndm, dms.data(), c.centre_frequency, c.bandwidth,
+                               &tu, nullptr));
+            fft_len = tu.fft_len;
+            cb_tpi = tu.cb_tiles_per_item;
         } else {
-            double best = 1e30;
-            for(int n = 1024; n <= 8192; n *= 2) {
-                if(n <= overlap) continue;
-                const double cost = std::log2((double)n) / (1.0 - (double)overlap / n);
-                if(cost < best - 1e-9) { best = cost; fft_len = n; }
-            }
+            fft_len = swb::cdd_model_fft_len(overlap);
         }
         SW_REQUIRE(fft_len > overlap && fft_len >= 256 && fft_len <= 65536,
                    "pipeline: fft_len %d does not exceed the DM smear of %d samples or is "
@@ -265,7 +260,7 @@ int sw_pipeline::enqueue_chain(const void* d_in, int parity, bool first)
                                       ib_raw[parity][d].as<float>(),
                                       ib_i8[parity][d].as<int8_t>(), ss));
     }
-    sw_cb_shape shape{F, T, A, B, ts, cfg.stokes, cfg.ib_subtract, vstride, voff};
+    sw_cb_shape shape{F, T, A, B, ts, cfg.stokes, cfg.ib_subtract, vstride, voff, cb_tpi};
     if(cfg.grouped) {
         // one problem per DM over all beams: the epilogue resolves each beam's
         // beamset (scale, offset, IB power) itself, so 128-beam tiles pack

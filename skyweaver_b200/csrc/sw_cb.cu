@@ -39,7 +39,7 @@ constexpr int kTileT       = 64;   // samples per tile
 constexpr int kN           = 2 * kTileT;
 constexpr int kVStages     = 4;
 constexpr int kWStages     = 2;
-constexpr int kTilesPerItem = 16;  // 1024 samples of one channel per item
+constexpr int kTilesPerItem = 16;  // default work item: 1024 samples of one channel
 constexpr int kMaxDm       = 16;
 constexpr int kMaxProblems = 96;
 // Epilogue warps: four per TMEM lane quarter, each owning 16 samples of a
@@ -65,7 +65,7 @@ struct Params {
     Problem prob[kMaxProblems];
     int nproblems, nitems;
     int nchans, nsamples, nant, nbeams, tscrunch, stokes, ib_subtract;
-    int kbytes, ntc;
+    int kbytes, ntc, tpi;
     size_t sample_offset;
     const float* scale;
     const float* offset;
@@ -408,8 +408,8 @@ cb_kernel(const __grid_constant__ Params P)
                 tma_load_2d(wdst, &P.wmap, &w_full[ws], 0, (it.f * 2 + 0) * P.nbeams + it.b0);
                 tma_load_2d(wdst + wtile, &P.wmap, &w_full[ws], 0, (it.f * 2 + 1) * P.nbeams + it.b0);
                 if(++ws == kWStages) { ws = 0; wph ^= 1; }
-                const int tile0 = it.tc * kTilesPerItem;
-                const int tile1 = min(ntiles_gulp, tile0 + kTilesPerItem);
+                const int tile0 = it.tc * P.tpi;
+                const int tile1 = min(ntiles_gulp, tile0 + P.tpi);
                 for(int tile = tile0; tile < tile1; ++tile) {
                     if(!mbar_wait(&v_empty[vs], vph ^ 1, s_abort, deadline, P.err)) break;
                     mbar_expect_tx(&v_full[vs], vtile);
@@ -429,8 +429,8 @@ cb_kernel(const __grid_constant__ Params P)
                 const Item it = decode(P, item);
                 if(!mbar_wait(&w_full[ws], wph, s_abort, deadline, P.err)) break;
                 const uint32_t wa = smem_u32(wbuf + ws * 2 * wtile);
-                const int tile0 = it.tc * kTilesPerItem;
-                const int tile1 = min(ntiles_gulp, tile0 + kTilesPerItem);
+                const int tile0 = it.tc * P.tpi;
+                const int tile1 = min(ntiles_gulp, tile0 + P.tpi);
                 bool ok = true;
                 for(int tile = tile0; tile < tile1; ++tile) {
                     if(!mbar_wait(&v_full[vs], vph, s_abort, deadline, P.err)) { ok = false; break; }
@@ -462,7 +462,10 @@ cb_kernel(const __grid_constant__ Params P)
     } else {
         // ------------------------------------------------------ epilogue
         constexpr int kSlice  = TS > 16 ? 32 : 16;   // samples per warp per tile
-        constexpr int kGroups = kSlice / 8;          // x8 column groups per warp
+        // 8 TMEM columns per load group: x16 groups need more registers than
+        // the 18-warp launch leaves (they spill at the 96 the launch allows)
+        constexpr int kG      = 8;
+        constexpr int kGroups = kSlice / kG;         // column groups per warp
         const int q = warp & 3;          // TMEM lane quarter of this warp
         const int h = (warp - 2) >> 2;   // which slice of the tile's 64 samples
         const int F = P.nchans;
@@ -482,8 +485,8 @@ cb_kernel(const __grid_constant__ Params P)
             const int bs = valid ? P.mapping[b] : 0;
             const float scale = P.scale[bs * F + it.f];
             const float offs  = P.offset[bs * F + it.f];
-            const int tile0 = it.tc * kTilesPerItem;
-            const int tile1 = min(ntiles_gulp, tile0 + kTilesPerItem);
+            const int tile0 = it.tc * P.tpi;
+            const int tile1 = min(ntiles_gulp, tile0 + P.tpi);
             bool ok = true;
             constexpr int NC = STOKES == 4 ? 4 : 1;  // output components
             // IB powers of this warp's outputs in the tile, fetched before the
@@ -515,17 +518,24 @@ cb_kernel(const __grid_constant__ Params P)
                 for(int c = 0; c < NC; ++c) power[c] = 0.0f;
 #pragma unroll
                 for(int g = 0; g < kGroups; ++g) {
-                    const uint32_t ta = lane_base + ab * 256 + h * kSlice + g * 8;
-                    uint32_t r0[8], r1[8], i0[8], i1[8];
-                    SW_TMEM_LD8(ta, r0);
-                    SW_TMEM_LD8(ta + 64, r1);
-                    SW_TMEM_LD8(ta + 128, i0);
-                    SW_TMEM_LD8(ta + 192, i1);
+                    const uint32_t ta = lane_base + ab * 256 + h * kSlice + g * kG;
+                    uint32_t r0[kG], r1[kG], i0[kG], i1[kG];
+                    if constexpr(kG == 16) {
+                        SW_TMEM_LD16(ta, r0);
+                        SW_TMEM_LD16(ta + 64, r1);
+                        SW_TMEM_LD16(ta + 128, i0);
+                        SW_TMEM_LD16(ta + 192, i1);
+                    } else {
+                        SW_TMEM_LD8(ta, r0);
+                        SW_TMEM_LD8(ta + 64, r1);
+                        SW_TMEM_LD8(ta + 128, i0);
+                        SW_TMEM_LD8(ta + 192, i1);
+                    }
                     tmem_wait_ld();
-                    const int tbase = tile * kTileT + h * kSlice + g * 8;
+                    const int tbase = tile * kTileT + h * kSlice + g * kG;
                     if(P.debug != nullptr && valid) {
                         int2* dbg = reinterpret_cast<int2*>(P.debug);
-                        for(int t = 0; t < 8; ++t) {
+                        for(int t = 0; t < kG; ++t) {
                             const size_t base_t = (size_t)it.f * P.nsamples + tbase + t;
                             dbg[(base_t * 2 + 0) * P.nbeams + b] =
                                 make_int2((int)r0[t], (int)i0[t]);
@@ -533,14 +543,14 @@ cb_kernel(const __grid_constant__ Params P)
                                 make_int2((int)r1[t], (int)i1[t]);
                         }
                     }
-                    float st[NC][8];
-                    if constexpr(STOKES == 4) stokes_iquv<8>(r0, r1, i0, i1, st);
-                    else stokes_n<STOKES, 8>(r0, r1, i0, i1, st[0]);
+                    float st[NC][kG];
+                    if constexpr(STOKES == 4) stokes_iquv<kG>(r0, r1, i0, i1, st);
+                    else stokes_n<STOKES, kG>(r0, r1, i0, i1, st[0]);
 #pragma unroll
-                    for(int t = 0; t < 8; ++t) {
+                    for(int t = 0; t < kG; ++t) {
 #pragma unroll
                         for(int c = 0; c < NC; ++c) power[c] = fadd(power[c], st[c][t]);
-                        const int u = g * 8 + t;  // sample within this warp's slice
+                        const int u = g * kG + t;  // sample within this warp's slice
                         const bool emit = ((u + 1) % TS) == 0;
                         if(emit) {
                             const int to = (tbase + t) / TS;
@@ -714,7 +724,10 @@ int launch(const sw_cb_shape* s, const sw_cb_problem* probs, int nprob,
     memset(&P, 0, sizeof(P));
     const void* dms[kMaxDm];
     int ndm = 0, item = 0;
-    const int ntc = cdiv(s->nsamples / kTileT, kTilesPerItem);
+    SW_REQUIRE(s->tiles_per_item >= 0 && s->tiles_per_item <= 1024,
+               "CoherentBeamformer: tiles_per_item must be in [0, 1024]");
+    const int tpi = s->tiles_per_item > 0 ? s->tiles_per_item : kTilesPerItem;
+    const int ntc = cdiv(s->nsamples / kTileT, tpi);
     for(int i = 0; i < nprob; ++i) {
         const sw_cb_problem& pr = probs[i];
         SW_REQUIRE(pr.d_fpact && pr.d_out && (pr.d_ib_raw || !s->ib_subtract),
@@ -756,6 +769,7 @@ int launch(const sw_cb_shape* s, const sw_cb_problem* probs, int nprob,
     P.ib_subtract = s->ib_subtract;
     P.kbytes      = 2 * s->nantennas;
     P.ntc         = ntc;
+    P.tpi = tpi;
     P.sample_offset = s->sample_offset;
     P.scale   = scale;
     P.offset  = offset;

@@ -235,6 +235,19 @@ def incoherent_dedisperse(tfb, delays, max_delay, tscrunch, scale_factor, stream
     return out
 
 
+def autotune(nantennas, nbeams, nchans, nsamples, tscrunch, dms, centre_frequency, bandwidth,
+             stream=None):
+    """sw_autotune: the fastest FFT length and beamformer work-item size for
+    this shape, measured on the device (cached per shape for the process)."""
+    t = _lib.Tuning()
+    d = (ctypes.c_float * len(dms))(*[float(x) for x in dms])
+    call("sw_autotune", nantennas, nbeams, nchans, nsamples, tscrunch, len(dms), d,
+         ctypes.c_double(centre_frequency), ctypes.c_double(bandwidth), ctypes.byref(t),
+         _stream(stream))
+    return {"fft_len": t.fft_len, "overlap": t.overlap, "cb_tiles_per_item": t.cb_tiles_per_item,
+            "cdd_ms": t.cdd_ms, "cb_ms": t.cb_ms}
+
+
 class IncoherentDedispersionPipeline:
     """IncoherentDedispersionPipeline (detail/IncoherentDedispersionPipeline.cu:
     6-113) with its AggregationBuffer (detail/AggregationBuffer.cu:23-117) in
@@ -285,7 +298,8 @@ class BeamformerPipeline:
     def __init__(self, *, nantennas, input_nantennas, nchans, nbeams, gulp_samples,
                  tscrunch, centre_frequency, bandwidth, dms, beamset_weights,
                  beamset_mapping, stokes="I", ib_subtract=True, output_level=24.0,
-                 fft_len=0, coherent_dedispersion=True, grouped=True, use_graph=True):
+                 fft_len=0, coherent_dedispersion=True, grouped=True, use_graph=True,
+                 autotune=False):
         self._dms = (ctypes.c_float * len(dms))(*[float(d) for d in dms])
         bw = np.ascontiguousarray(beamset_weights, np.float32)
         mp = np.ascontiguousarray(beamset_mapping, np.int32)
@@ -296,7 +310,7 @@ class BeamformerPipeline:
             nantennas, input_nantennas, nchans, nbeams, gulp_samples, tscrunch,
             STOKES[stokes], int(ib_subtract), output_level, centre_frequency, bandwidth,
             len(dms), self._dms, fft_len, int(coherent_dedispersion), int(grouped),
-            int(use_graph), bw.shape[0], self._bw, self._mp)
+            int(use_graph), bw.shape[0], self._bw, self._mp, int(autotune))
         h = ctypes.c_void_p()
         call("sw_pipeline_create", ctypes.byref(cfg), ctypes.byref(h))
         self.h = h

@@ -220,3 +220,40 @@ def test_dispersed_pulse_peaks_in_its_dm_fft65536(cuda, oracle):
     # re-compressed: the DM 150 peak stands well above its own noise
     s = series[2]
     assert (s.max() - np.median(s)) > 6 * s.std()
+
+
+def test_autotune_choices_and_results(cuda, oracle):
+    """sw_autotune picks a valid FFT length and beamformer work-item size for
+    the shape, caches it, and a pipeline built with autotune gives the same
+    beams as the default plan (DM 0 is exact for any FFT length; the
+    work-item size never changes results)."""
+    torch = cuda
+    import time
+    from skyweaver_b200 import stages, synthetic
+    g = synthetic.rng(91)
+    A, F, B, T, ts = 32, 4, 256, 8192, 16
+    chbw = 856e6 / 1024
+    centre, bw = 1284e6, F * chbw
+    dms = [0.0, 150.0]
+    t = stages.autotune(A, B, F, T, ts, dms, centre, bw)
+    assert t["fft_len"] > t["overlap"] and t["fft_len"] & (t["fft_len"] - 1) == 0
+    assert t["cb_tiles_per_item"] in (4, 8, 16, 32, 64)
+    assert t["cdd_ms"] > 0 and t["cb_ms"] > 0
+    t0 = time.perf_counter()
+    assert stages.autotune(A, B, F, T, ts, dms, centre, bw) == t      # cached
+    assert time.perf_counter() - t0 < 0.05
+    taftp = synthetic.voltages_taftp(g, T // 256, A, F, sigma=8)
+    delays = synthetic.delay_model(g, B, A)
+    outs = []
+    for tune in (False, True):
+        pipe = stages.BeamformerPipeline(nantennas=A, input_nantennas=A, nchans=F, nbeams=B,
+                                         gulp_samples=T, tscrunch=ts, centre_frequency=centre,
+                                         bandwidth=bw, dms=dms, beamset_weights=np.ones((1, A)),
+                                         beamset_mapping=np.zeros(B, np.int32), autotune=tune)
+        if tune:
+            assert pipe.fft_plan()[0] == t["fft_len"]
+        pipe.set_delays(delays, 1.7e9)
+        pipe.process_device(torch.from_numpy(taftp).cuda(), 1.7e9)
+        outs.append(pipe.outputs(0)["cb"])
+        pipe.close()
+    assert np.array_equal(outs[0], outs[1])
