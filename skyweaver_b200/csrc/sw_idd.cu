@@ -22,24 +22,36 @@ __device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel)
     return d;
 }
 
-// grid: x = beam quads, y = output samples, z = trial DMs
-__global__ void idd_k(const uint32_t* __restrict__ tfb, int nchans, int nquads,
-                      const int* __restrict__ delays, int max_delay,
-                      int tscrunch, float scale_factor,
-                      uint32_t* __restrict__ tdb, int ndms, int nout)
+// One CTA = (trial DM, output sample, block of 128 beam quads).  The linear
+// block index runs over the DMs of a group of `group` DMs fastest, then
+// output samples, then beam-quad blocks, then DM groups, so the CTAs resident
+// at any moment are neighbouring DMs at neighbouring times of one 512-beam
+// block: they read nearly the same (time - delay) rows of every channel, a
+// window that fits in L2, instead of streaming the rows from HBM once per DM.
+__global__ void __launch_bounds__(128)
+idd_k(const uint32_t* __restrict__ tfb, int nchans, int nquads,
+      const int* __restrict__ delays, int max_delay, int tscrunch,
+      float scale_factor, uint32_t* __restrict__ tdb, int ndms, int nout,
+      int nqb, int group, long long blk0)
 {
-    const int q  = blockIdx.x * blockDim.x + threadIdx.x;
-    const int to = blockIdx.y;
-    const int d  = blockIdx.z;
-    if(q >= nquads || to >= nout) return;
+    long long blk = blk0 + blockIdx.x;
+    const int dl = (int)(blk % group);
+    blk /= group;
+    const int to = (int)(blk % nout);
+    blk /= nout;
+    const int qb = (int)(blk % nqb);
+    const int d  = (int)(blk / nqb) * group + dl;
+    const int q  = qb * blockDim.x + threadIdx.x;
+    if(d >= ndms || q >= nquads) return;
     const int t = max_delay + to * tscrunch;
-    const int* dl = delays + (size_t)d * nchans;
+    const int* dl_f = delays + (size_t)d * nchans;
     int acc[4] = {0, 0, 0, 0};
     uint32_t lo = 0, hi = 0;
     int pending = 0;
     for(int tau = 0; tau < tscrunch; ++tau) {
+#pragma unroll 4
         for(int f = 0; f < nchans; ++f) {
-            const size_t row = (size_t)(t + tau - dl[f]) * nchans + f;
+            const size_t row = (size_t)(t + tau - dl_f[f]) * nchans + f;
             const uint32_t w = tfb[row * nquads + q] ^ 0x80808080u;
             lo += prmt(w, 0, 0x4240);  // bytes 0,2 -> 16-bit lanes
             hi += prmt(w, 0, 0x4341);  // bytes 1,3
@@ -63,6 +75,75 @@ __global__ void idd_k(const uint32_t* __restrict__ tfb, int nchans, int nquads,
     tdb[((size_t)to * ndms + d) * nquads + q] = packed;
 }
 
+// Same sums, four beam quads (16 beams, one 16-byte load) per thread: the
+// per-load address work is shared by 16 beams and each channel's row offset
+// comes from a per-CTA table in shared memory.  Needs nbeams % 16 == 0 and
+// 16-byte aligned buffers.  Block order as idd_k.
+__global__ void __launch_bounds__(128)
+idd16_k(const uint4* __restrict__ tfb, int nchans, int nq16,
+        const int* __restrict__ delays, int max_delay, int tscrunch,
+        float scale_factor, uint4* __restrict__ tdb, int ndms, int nout,
+        int nqb, int group, long long blk0)
+{
+    extern __shared__ long long s_off[];  // [nchans] row offsets in uint4 units
+    long long blk = blk0 + blockIdx.x;
+    const int dl = (int)(blk % group);
+    blk /= group;
+    const int to = (int)(blk % nout);
+    blk /= nout;
+    const int qb = (int)(blk % nqb);
+    const int d  = (int)(blk / nqb) * group + dl;
+    if(d >= ndms) return;  // uniform across the CTA
+    const int* dl_f = delays + (size_t)d * nchans;
+    const long long row = (long long)nchans * nq16;  // uint4 per time sample
+    for(int f = threadIdx.x; f < nchans; f += blockDim.x)
+        s_off[f] = (long long)f * nq16 - (long long)dl_f[f] * row;
+    __syncthreads();
+    const int q = qb * blockDim.x + threadIdx.x;
+    if(q >= nq16) return;
+    const int t = max_delay + to * tscrunch;
+    int acc[16];
+#pragma unroll
+    for(int k = 0; k < 16; ++k) acc[k] = 0;
+    for(int tau = 0; tau < tscrunch; ++tau) {
+        const uint4* bt = tfb + (long long)(t + tau) * row + q;
+        for(int f0 = 0; f0 < nchans; f0 += 256) {
+            const int f1 = min(nchans, f0 + 256);
+            uint32_t lo[4] = {0, 0, 0, 0}, hi[4] = {0, 0, 0, 0};
+#pragma unroll 4
+            for(int f = f0; f < f1; ++f) {
+                const uint4 v = bt[s_off[f]];
+                const uint32_t w[4] = {v.x ^ 0x80808080u, v.y ^ 0x80808080u,
+                                       v.z ^ 0x80808080u, v.w ^ 0x80808080u};
+#pragma unroll
+                for(int k = 0; k < 4; ++k) {
+                    lo[k] += prmt(w[k], 0, 0x4240);  // bytes 0,2 -> 16-bit lanes
+                    hi[k] += prmt(w[k], 0, 0x4341);  // bytes 1,3
+                }
+            }
+#pragma unroll
+            for(int k = 0; k < 4; ++k) {  // at most 256 adds of <= 255 per lane
+                acc[4 * k + 0] += (int)(lo[k] & 0xffff);
+                acc[4 * k + 2] += (int)(lo[k] >> 16);
+                acc[4 * k + 1] += (int)(hi[k] & 0xffff);
+                acc[4 * k + 3] += (int)(hi[k] >> 16);
+            }
+        }
+    }
+    const int bias = 128 * tscrunch * nchans;
+    uint32_t packed[4];
+#pragma unroll
+    for(int k = 0; k < 4; ++k) {
+        packed[k] = 0;
+#pragma unroll
+        for(int b = 0; b < 4; ++b) {
+            const float v = fdiv((float)(acc[4 * k + b] - bias), scale_factor);
+            packed[k] |= ((uint32_t)(uint8_t)clamp_i8(v)) << (8 * b);
+        }
+    }
+    tdb[((size_t)to * ndms + d) * nq16 + q] = make_uint4(packed[0], packed[1], packed[2], packed[3]);
+}
+
 }  // namespace
 }  // namespace swb
 
@@ -81,18 +162,28 @@ extern "C" int sw_incoherent_dedisperse(const int8_t* d_tfb, int nsamples,
     SW_REQUIRE(nbeams % 4 == 0, "sw_incoherent_dedisperse: nbeams must be a multiple of 4");
     SW_REQUIRE(ndms > 0 && ndms <= 65535, "sw_incoherent_dedisperse: bad DM count");
     const int nout = (nsamples - max_delay) / tscrunch;
-    SW_REQUIRE(nout <= 65535 * 1024, "sw_incoherent_dedisperse: too many samples");
     const int nquads = nbeams / 4;
-    // nout may exceed the 65535 y-grid limit: chunk the launch over y
-    for(int base = 0; base < nout; base += 65535) {
-        const int n = nout - base < 65535 ? nout - base : 65535;
-        dim3 grid(swb::cdiv(nquads, 128), n, ndms);
-        swb::idd_k<<<grid, 128, 0, swb::as_cuda(stream)>>>(
-            reinterpret_cast<const uint32_t*>(d_tfb) +
-                (size_t)base * tscrunch * nchans * nquads,
-            nchans, nquads, d_delays, max_delay, tscrunch, scale_factor,
-            reinterpret_cast<uint32_t*>(d_tdb) + (size_t)base * ndms * nquads,
-            ndms, n);
+    const bool wide = nbeams % 16 == 0 && (reinterpret_cast<uintptr_t>(d_tfb) & 15) == 0 &&
+                      (reinterpret_cast<uintptr_t>(d_tdb) & 15) == 0 &&
+                      (size_t)nchans * sizeof(long long) <= 48 * 1024;
+    const int nlanes = wide ? nbeams / 16 : nquads;  // threads per (DM, sample)
+    const int nqb = swb::cdiv(nlanes, 128);
+    const int group = ndms < 16 ? ndms : 16;
+    const long long ngroups = swb::cdiv(ndms, group);
+    const long long total = ngroups * nout * nqb * group;
+    const long long chunk = 1ll << 30;  // blocks per launch (grid.x limit 2^31 - 1)
+    for(long long b0 = 0; b0 < total; b0 += chunk) {
+        const long long n = total - b0 < chunk ? total - b0 : chunk;
+        if(wide)
+            swb::idd16_k<<<(unsigned)n, 128, nchans * sizeof(long long), swb::as_cuda(stream)>>>(
+                reinterpret_cast<const uint4*>(d_tfb), nchans, nlanes, d_delays, max_delay,
+                tscrunch, scale_factor, reinterpret_cast<uint4*>(d_tdb), ndms, nout, nqb,
+                group, b0);
+        else
+            swb::idd_k<<<(unsigned)n, 128, 0, swb::as_cuda(stream)>>>(
+                reinterpret_cast<const uint32_t*>(d_tfb), nchans, nquads, d_delays, max_delay,
+                tscrunch, scale_factor, reinterpret_cast<uint32_t*>(d_tdb), ndms, nout, nqb,
+                group, b0);
         SW_LAUNCH_CHECK();
     }
     return SW_OK;
