@@ -257,3 +257,103 @@ def test_autotune_choices_and_results(cuda, oracle):
         outs.append(pipe.outputs(0)["cb"])
         pipe.close()
     assert np.array_equal(outs[0], outs[1])
+
+
+def test_uhf_pipeline_with_incoherent_dedispersion_vs_oracle(cuda, oracle):
+    """UHF end-to-end chain, reduced: 16 channels at the top of the 544-1088
+    MHz band (1024-channel mode), 16 antennas, 32 beams, coherent DMs {0, 300},
+    tscrunch 8, then the device incoherent-dedispersion pipeline with 9 trial
+    DMs around each coherent DM.  A pulse dispersed at DM 300 (intra-channel
+    by the conjugate DM 300 response, inter-channel by the incoherent delays)
+    arrives at boresight.  The GPU TDB must match the oracle chain (exact for
+    the DM 0 block, within one LSB on a small fraction for DM 300), and both
+    must recover the pulse at the trial nearest DM 300 with the same S/N."""
+    torch = cuda
+    from skyweaver_b200 import stages, synthetic
+    g = synthetic.rng(300)
+    A, F, B, T, ts = 16, 16, 32, 32768, 8
+    chbw = 0.53125e6
+    top = 1088e6
+    bw = F * chbw
+    centre = top - bw / 2
+    low = float(np.float32(centre - bw / 2))
+    freqs = synthetic.channel_frequencies(centre, bw, F)
+    coh = [0.0, 300.0]
+    trials = [np.linspace(-10, 10, 9).astype(np.float32) + c for c in coh]
+    trials[0] = np.abs(trials[0])
+    cb_tsamp = ts / chbw
+    idd = [oracle.idd_delays(freqs, tr, cb_tsamp) for tr in trials]
+    # the pulse: 64 raw samples, lowest channel at raw time t_low
+    maxd1 = idd[1][1]
+    t_low = 8 * (maxd1 + 900)
+    v = g.normal(0, 8, size=(F, T, 2, A, 2))
+    H = oracle.chirp(F, T, low, bw, 300.0)
+    k = 4.148806423e15
+    for c in range(F):
+        shift = int(round(k * 300.0 * (1 / freqs[0] ** 2 - 1 / freqs[c] ** 2) * chbw))
+        burst = np.zeros(T, np.complex128)
+        burst[t_low - shift: t_low - shift + 64] = 6.0
+        disp = np.fft.ifft(np.fft.fft(burst) * np.conj(H[c]))
+        v[c, :, :, :, 0] += disp.real[:, None, None]
+        v[c, :, :, :, 1] += disp.imag[:, None, None]
+    ftpa = np.clip(np.rint(v), -127, 127).astype(np.int8)
+    taftp = ftpa.reshape(F, T // 256, 256, 2, A, 2).transpose(1, 4, 0, 2, 3, 5).copy()
+    delays = synthetic.delay_model(g, B, A)
+    delays[0] = [1.0, 0.0, 0.0]                  # beam 0 at boresight
+    bw1 = np.ones((1, A), np.float32)
+    mapping = np.zeros(B, np.int32)
+    pipe = stages.BeamformerPipeline(nantennas=A, input_nantennas=A, nchans=F, nbeams=B,
+                                     gulp_samples=T, tscrunch=ts, centre_frequency=centre,
+                                     bandwidth=bw, dms=coh, beamset_weights=bw1,
+                                     beamset_mapping=mapping)
+    fft_len, overlap = pipe.fft_plan()
+    pipe.set_delays(delays, 1.7e9)
+    pipe.process_device(torch.from_numpy(taftp).cuda(), 1.7e9)
+    cbs = [pipe.outputs(d)["cb"] for d in range(2)]
+    pipe.close()
+    sf = [float(np.float32(math.sqrt(F * 1))) for _ in coh]
+    got = {0: [], 1: []}
+    idp = stages.IncoherentDedispersionPipeline(
+        F, B, [(idd[b][0], 1, sf[b]) for b in range(2)],
+        lambda b, t: got[b].append(t.cpu().numpy()), dispatch=[2048, 2048])
+    for d in range(2):
+        idp.push(d, torch.from_numpy(np.ascontiguousarray(cbs[d])).cuda())
+    idp.close()
+    # oracle chain
+    ext = np.concatenate([np.zeros((F, overlap, 2, A, 2), np.int8), ftpa], axis=1)
+    scl = oracle.scalings(oracle.statistics(ftpa), bw1, 1, ts, ts, 24.0)
+    w = oracle.weights(delays, freqs, 1.7e9, 1.7e9)
+    snr = []
+    for d, dm in enumerate(coh):
+        dd = oracle.cdd_ftpa(ext, T, oracle.chirp(F, fft_len, low, bw, dm), overlap)
+        cb_ref = oracle.coherent_beam(dd, w, ts, scl[1], scl[0], bw1, mapping)
+        if d == 0:
+            assert np.array_equal(cbs[0], cb_ref)
+        else:
+            diff = np.abs(cbs[1].astype(int) - cb_ref.astype(int))
+            assert diff.max() <= 1 and (diff > 0).mean() < 2e-3
+        delays_d, maxd = idd[d]
+        D = 2048
+        assert len(got[d]) == 1
+        ref = oracle.idd(np.ascontiguousarray(cb_ref[:D + maxd]), delays_d, maxd, 1, sf[d])
+        tdb = got[d][0]
+        if d == 0:
+            assert np.array_equal(tdb, ref)
+        else:
+            diff = np.abs(tdb.astype(int) - ref.astype(int))
+            assert (diff > 0).mean() < 2e-2, (diff > 0).mean()
+        row = []
+        for arr in (tdb, ref):
+            # boresight beam, 8-sample boxcar (the pulse width): int8 outputs
+            # saturate at 127, so single samples cap the S/N near 5
+            s = arr[:, :, 0].astype(np.float64)          # [t][trial]
+            s = np.stack([np.convolve(s[:, j], np.ones(8), "valid") for j in range(s.shape[1])], 1)
+            base = np.median(s, axis=0)
+            noise = s.std(axis=0)
+            row.append(((s - base) / noise).max(axis=0))
+        snr.append(row)
+    gpu, cpu = snr[1]
+    best = int(np.argmax(gpu))
+    print("DM 300 block S/N per trial: gpu", np.round(gpu, 1), "cpu", np.round(cpu, 1))
+    assert best == int(np.argmin(np.abs(trials[1] - 300.0)))
+    assert gpu[best] > 8 and abs(gpu[best] - cpu[best]) < 0.05 * cpu[best]
