@@ -21,6 +21,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import subprocess
 import sys
@@ -325,11 +326,13 @@ def main_b200(args):
             "batched_vs_plain": ms_plain / ms_graph, "ragged": ragged,
             "kernels": kern, "roofline": roof, "hbm_peak_gbs": hbm_peak, "e2e": e2e,
             "gpu_launches": launches * args.steps, "clocks": clocks}
+    pipe.close()
+    if not args.no_uhf:
+        line["uhf"] = uhf_case(torch, stages, synthetic, max(8, (args.steps + 3) // 4 * 4), 8)
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = {k: v for k, v in cpu_baseline().items() if k != "seconds"}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    pipe.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -480,6 +483,80 @@ def ragged_case(torch, stages, synthetic, K):
             "pipeline_grouped_vs_plain": res["plain_eager"] / res["grouped_graph"]}
 
 
+UHF = dict(nant=64, nchans=256, nbeams=2048, gulp=65536, tscrunch=8, coherent_dms=[0.0, 300.0],
+           ntrials=128, trial_span=50.0, chbw=856e6 / 1024 * 544 / 856, top=1088e6,
+           idd_dispatch=32768)
+
+
+def uhf_case(torch, stages, synthetic, K, W):
+    """End-to-end UHF chain: 64 antennas x 256 channels (the top of the
+    544-1088 MHz band in 1024-channel mode, 0.53125 MHz channels), 2048
+    coherent beams + incoherent beam, coherent DMs {0, 300}, tscrunch 8,
+    then on the device the incoherent-dedispersion pipeline with 128 trial
+    DMs over +-50 around each coherent DM (non-negative), dispatching every
+    32768 beamformed samples (4 gulps; the dispatch must cover the 24837-sample
+    overlap of the DM 250-350 block).  Times W + K gulps of synthetic voltages
+    and reports the steady-state real-time factor of the K timed gulps (a
+    multiple of 4, so each block dispatches K / 4 times inside them)."""
+    U = UHF
+    A, F, B, T, ts = U["nant"], U["nchans"], U["nbeams"], U["gulp"], U["tscrunch"]
+    chbw = U["chbw"]
+    bw = F * chbw
+    centre = U["top"] - bw / 2
+    freqs = stages.channel_frequencies(centre, bw, F)
+    g = synthetic.rng(1088)
+    delays = synthetic.delay_model(g, B, A)
+    pipe = stages.BeamformerPipeline(nantennas=A, input_nantennas=A, nchans=F, nbeams=B,
+                                     gulp_samples=T, tscrunch=ts, centre_frequency=centre,
+                                     bandwidth=bw, dms=U["coherent_dms"],
+                                     beamset_weights=np.ones((1, A), np.float32),
+                                     beamset_mapping=np.zeros(B, np.int32))
+    pipe.set_delays(delays, 1.7e9)
+    cb_tsamp = ts / chbw
+    k = 4.148806423e15
+    blocks = []
+    for dm in U["coherent_dms"]:
+        trials = np.abs(np.linspace(dm - U["trial_span"], dm + U["trial_span"], U["ntrials"]))
+        dl = np.array([[int(k * (1 / freqs[0] ** 2 - 1 / f ** 2) * d / cb_tsamp + 0.5)
+                        for f in freqs] for d in trials.astype(np.float32)], np.int32)
+        blocks.append((dl, 1, float(np.float32(math.sqrt(F)))))
+    idp = stages.IncoherentDedispersionPipeline(F, B, blocks, None,
+                                                dispatch=[U["idd_dispatch"]] * len(blocks))
+    gen = torch.Generator(device="cuda").manual_seed(4321)
+    taftp = (torch.randn((T // 256, A, F, 256, 2, 2), generator=gen, device="cuda") * 8.0)
+    taftp = taftp.round_().clamp_(-127, 127).to(torch.int8)
+    stream = torch.cuda.current_stream()
+
+    def gulp(i):
+        pipe.process_device(taftp, 1.7e9 + i * T / chbw)
+        for d in range(len(blocks)):
+            idp.push(d, pipe.cb_device(d))
+
+    for i in range(W):
+        gulp(i)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(K):
+        gulp(W + i)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / K
+    geo = [idp.geometry(b) for b in range(len(blocks))]
+    idp.close()
+    pipe.close()
+    del taftp
+    torch.cuda.empty_cache()
+    gulp_s = T / chbw
+    adds = sum(U["ntrials"] * (T // ts) * B * F for _ in blocks)
+    return {"workload": "UHF 544-1088 MHz (top 256 of 1024 channels), 64 ant x 2048 beams, "
+                        "coherent DMs {0,300}, tscrunch 8, 128 incoherent trials per coherent "
+                        "DM over +-50, device aggregation (dispatch 32768)",
+            "ms_per_gulp": ms, "rtf": gulp_s / (ms * 1e-3),
+            "idd_adds_per_gulp": adds, "idd_overlap_samples": [g[1] for g in geo],
+            "timed_gulps": K, "warmup_gulps": W}
+
+
 def profile_case(which, nchans=16, reps=3):
     """Small single-kernel case for ncu captures: `nchans` channels of the
     benchmark workload (268 MB of voltages for 16 channels, above L2), one
@@ -526,6 +603,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-uhf", action="store_true",
+                    help="skip the UHF beamforming + incoherent dedispersion measurement")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     args = ap.parse_args()
     if args.profile:

@@ -266,10 +266,11 @@ class IncoherentDedispersionPipeline:
         ts = (ctypes.c_int * nb)(*[int(b[1]) for b in blocks])
         sc = (ctypes.c_float * nb)(*[float(b[2]) for b in blocks])
         disp = (ctypes.c_int * nb)(*dispatch) if dispatch is not None else None
-        self._cb = _lib.IDD_HANDLER(self._on_dispatch)
+        self._cb = _lib.IDD_HANDLER(self._on_dispatch) if handler is not None else None
         h = ctypes.c_void_p()
         call("sw_idd_pipeline_create", nchans, nbeams, nb, ndms, dptr, ts, sc, disp,
-             ctypes.cast(self._cb, ctypes.c_void_p), None, ctypes.byref(h))
+             ctypes.cast(self._cb, ctypes.c_void_p) if self._cb is not None else None, None,
+             ctypes.byref(h))
         self.h = h
 
     def _on_dispatch(self, user, block, ptr, nout, ndms, nbeams, stream):
@@ -349,6 +350,15 @@ class BeamformerPipeline:
         n, o = ctypes.c_int(), ctypes.c_int()
         call("sw_pipeline_fft_len", self.h, ctypes.byref(n), ctypes.byref(o))
         return n.value, o.value
+
+    def cb_device(self, dm_idx: int):
+        """The last gulp's coherent beams of one DM as a device tensor view
+        (int8 TFB, owned by the pipeline, overwritten by the next gulp)."""
+        pcb = ctypes.c_void_p()
+        call("sw_pipeline_outputs", self.h, dm_idx, ctypes.byref(pcb), None, None, None)
+        T = self.gulp // self.tscrunch
+        shape = (T, self.nchans, self.nbeams) + ((4,) if self.stokes == "IQUV" else ())
+        return _device_view(pcb.value, int(np.prod(shape))).view(torch.int8).reshape(shape)
 
     def cb_bytes_per_dm(self):
         return lib().sw_pipeline_cb_bytes_per_dm(self.h)
