@@ -345,6 +345,60 @@ int sw_autotune(int nantennas, int nbeams, int nchans, int nsamples,
                 sw_stream_t stream);
 
 /* ------------------------------------------------------------------ */
+/* DADA ingest and output (host I/O around the pipeline)                */
+/* ------------------------------------------------------------------ */
+/* ObservationHeader (cpp/skyweaver/ObservationHeader.hpp:9-34); the
+ * reference's long double fields are double here (the raw strings stay
+ * available through sw_dada_header_get). */
+typedef struct sw_observation_header {
+    size_t nchans, npol, nbits, nantennas, sample_clock_start, chan0_idx;
+    size_t obs_nchans, obs_offset;
+    double bandwidth, obs_bandwidth, frequency, obs_frequency, tsamp;
+    double sample_clock, sync_time, utc_start, mjd_start;
+    char source_name[64], ra[32], dec[32], telescope[32], instrument[32];
+} sw_observation_header;
+
+/* Header::get (cpp/skyweaver/src/Header.cpp:26-70): the value of `key` at
+ * the start of a header line; errors on a missing key or "unset". */
+int sw_dada_header_get(const char* header, size_t header_size, const char* key,
+                       char* value, size_t value_capacity);
+/* read_dada_header (cpp/skyweaver/src/ObservationHeader.cpp:6-33). */
+int sw_dada_parse_header(const char* header, size_t header_size,
+                         sw_observation_header* out);
+/* validate_header (cpp/skyweaver/src/ObservationHeader.cpp:35-62). */
+int sw_dada_validate_header(const sw_observation_header* h, int nantennas,
+                            int nchans, int npol);
+
+/* MultiFileReader (cpp/skyweaver/src/MultiFileReader.cu:34-303): several
+ * DADA files read as one contiguous payload (headers skipped), with the
+ * optional OBS_OFFSET contiguity check; positions are payload bytes. */
+typedef struct sw_dada_reader sw_dada_reader;
+int sw_dada_reader_open(const char* const* files, int nfiles, size_t header_size,
+                        int check_contiguity, sw_dada_reader** out);
+void sw_dada_reader_close(sw_dada_reader* r);
+int sw_dada_reader_header(const sw_dada_reader* r, int file_idx,
+                          sw_observation_header* out);
+size_t sw_dada_reader_total_bytes(const sw_dada_reader* r);
+size_t sw_dada_reader_tell(const sw_dada_reader* r);
+int sw_dada_reader_seek(sw_dada_reader* r, size_t payload_offset);
+/* Reads up to `bytes` (fewer only at the end of the last file). */
+int sw_dada_reader_read(sw_dada_reader* r, void* dst, size_t bytes,
+                        size_t* nread);
+
+/* FileStream (cpp/skyweaver/src/FileOutputStream.cpp:80-150): a payload
+ * split over files of bytes_per_file payload bytes, each led by the header
+ * (template + sw_dada_writer_set keys) with FILE_SIZE, FILE_NUMBER and
+ * OBS_OFFSET updated, named <dir>/<base>_<offset %016zu><extension>. */
+typedef struct sw_dada_writer sw_dada_writer;
+int sw_dada_writer_open(const char* directory, const char* base_filename,
+                        const char* extension, size_t bytes_per_file,
+                        const char* header_template, size_t header_size,
+                        sw_dada_writer** out);
+int sw_dada_writer_set(sw_dada_writer* w, const char* key, const char* value);
+int sw_dada_writer_write(sw_dada_writer* w, const void* data, size_t bytes);
+int sw_dada_writer_close(sw_dada_writer* w);
+
+/* ------------------------------------------------------------------ */
 /* BeamformerPipeline                                                   */
 /* ------------------------------------------------------------------ */
 /* Replaces BeamformerPipeline<CBH,IBH,StatsH,BfTraits>

@@ -17,6 +17,10 @@
 #include <cstdint>
 #include <cstring>
 #include <fstream>
+#include <cctype>
+#include <ctime>
+#include <iomanip>
+#include <map>
 #include <memory>
 #include <sstream>
 #include <stdexcept>
@@ -624,6 +628,136 @@ class IncoherentDedispersionPipeline {
     Handler& _handler;
     std::vector<std::unique_ptr<IncoherentDedisperser>> _dedispersers;
     sw_idd_pipeline* _p = nullptr;
+};
+
+// ------------------------------------------------------------- DADA I/O
+// MultiFileReader (src/MultiFileReader.cu:34-303) over sw_dada_reader.
+class MultiFileReader {
+  public:
+    MultiFileReader(const std::vector<std::string>& files, std::size_t header_size = 4096,
+                    bool check_contiguity = false)
+    {
+        std::vector<const char*> names;
+        for(const auto& f : files) names.push_back(f.c_str());
+        check(sw_dada_reader_open(names.data(), (int)names.size(), header_size,
+                                  check_contiguity ? 1 : 0, &_r));
+    }
+    ~MultiFileReader() { sw_dada_reader_close(_r); }
+    MultiFileReader(const MultiFileReader&) = delete;
+    MultiFileReader& operator=(const MultiFileReader&) = delete;
+    sw_observation_header get_header(int file_idx = 0) const
+    {
+        sw_observation_header h{};
+        check(sw_dada_reader_header(_r, file_idx, &h));
+        return h;
+    }
+    std::size_t get_total_size() const { return sw_dada_reader_total_bytes(_r); }
+    std::size_t tellg() const { return sw_dada_reader_tell(_r); }
+    bool eof() const { return tellg() >= get_total_size(); }
+    void seekg(std::size_t pos) { check(sw_dada_reader_seek(_r, pos)); }
+    std::size_t read(char* dst, std::size_t bytes)
+    {
+        std::size_t got = 0;
+        check(sw_dada_reader_read(_r, dst, bytes, &got));
+        return got;
+    }
+
+  private:
+    sw_dada_reader* _r = nullptr;
+};
+
+// MultiFileWriter (detail/MultiFileWriter.cu:74-243): one size-split DADA
+// stream per stream index (coherent DM), the reference's directory and file
+// names and header keys.  Data is host memory.
+class MultiFileWriter {
+  public:
+    struct StreamInfo {
+        std::size_t nbeams, nchans, nsamples, ndms;
+        std::vector<float> dms;
+        float reference_dm;
+        double tsamp, utc_offset;
+        std::string dims;  // "TFB", "TDB", ...
+    };
+    MultiFileWriter(const std::string& output_dir, const sw_observation_header& header,
+                    std::size_t max_file_bytes, std::string stokes = "I", std::string prefix = "",
+                    std::string tag = "")
+        : _dir(output_dir), _h(header), _max(max_file_bytes), _stokes(std::move(stokes)),
+          _prefix(std::move(prefix)), _tag(std::move(tag))
+    {
+    }
+    ~MultiFileWriter()
+    {
+        for(auto& w : _w) sw_dada_writer_close(w.second);
+    }
+    void operator()(const int8_t* data, std::size_t bytes, const StreamInfo& s,
+                    std::size_t stream_idx)
+    {
+        auto it = _w.find(stream_idx);
+        if(it == _w.end()) it = _w.emplace(stream_idx, create(s, stream_idx, bytes)).first;
+        check(sw_dada_writer_write(it->second, data, bytes));
+    }
+
+  private:
+    static std::string utc(double t)
+    {
+        char b[80];
+        std::time_t u = (std::time_t)t;
+        std::strftime(b, sizeof(b), "%Y-%m-%d-%H:%M:%S", std::gmtime(&u));
+        return b;
+    }
+    sw_dada_writer* create(const StreamInfo& s, std::size_t idx, std::size_t block_bytes)
+    {
+        std::ostringstream dir, base, dims;
+        dir << _dir << "/" << utc(_h.utc_start) << "/" << idx << "/" << std::setfill('0')
+            << std::setw(9) << (long long)_h.frequency;
+        if(!_prefix.empty()) base << _prefix << "_";
+        base << utc(_h.utc_start) << "_" << idx << "_" << std::fixed << std::setprecision(3)
+             << std::setfill('0') << std::setw(9) << s.reference_dm << "_"
+             << std::setprecision(0) << std::setw(9) << _h.frequency;
+        if(!_tag.empty()) base << "_" << _tag;
+        std::string ext = "." + s.dims;
+        for(auto& c : ext) c = (char)std::tolower((unsigned char)c);
+        // file size rounded to a whole number of blocks (MultiFileWriter.cu:103-108)
+        const std::size_t filesize = std::max<std::size_t>(1, _max / block_bytes) * block_bytes;
+        sw_dada_writer* w = nullptr;
+        check(sw_dada_writer_open(dir.str().c_str(), base.str().c_str(), ext.c_str(), filesize,
+                                  nullptr, 4096, &w));
+        auto set = [&](const char* k, const std::string& v) { check(sw_dada_writer_set(w, k, v.c_str())); };
+        auto num = [](double v, int prec) {
+            std::ostringstream o;
+            o << std::fixed << std::setprecision(prec) << v;
+            return o.str();
+        };
+        set("NBEAM", std::to_string(s.nbeams));
+        set("NCHAN", std::to_string(s.nchans));
+        set("OBS_NCHAN", std::to_string(_h.obs_nchans));
+        set("OBS_FREQUENCY", num(_h.obs_frequency, 6));
+        set("OBS_BW", num(_h.obs_bandwidth, 6));
+        set("NSAMP", std::to_string(s.nsamples));
+        if(s.ndms) {
+            set("NDMS", std::to_string(s.ndms));
+            std::ostringstream d;
+            d << std::setprecision(7);
+            for(std::size_t i = 0; i < s.dms.size(); ++i) d << (i ? "," : "") << s.dms[i];
+            set("DMS", d.str());
+        }
+        set("COHERENT_DM", num(s.reference_dm, 6));
+        set("FREQ", num(_h.frequency, 6));
+        set("BW", num(_h.bandwidth, 6));
+        set("TSAMP", num(s.tsamp * 1e6, 6));
+        set("NPOL", _stokes == "IQUV" ? "4" : "1");
+        set("STOKES_MODE", _stokes);
+        set("ORDER", s.dims);
+        set("CHAN0_IDX", std::to_string(_h.chan0_idx));
+        set("OBS_OVERLAP", "0");
+        set("UTC_START", num(_h.utc_start + s.utc_offset, 6));
+        return w;
+    }
+    std::string _dir;
+    sw_observation_header _h;
+    std::size_t _max;
+    std::string _stokes, _prefix, _tag;
+    std::map<std::size_t, sw_dada_writer*> _w;
 };
 
 // -------------------------------------------------------- BeamformerPipeline

@@ -4,6 +4,7 @@
 // Built and run by tests/test_gpu_cpp_api.py.  Prints "PASS <name>" per case
 // and exits non-zero on the first failure.
 #include <cmath>
+#include <fstream>
 #include <cstdio>
 #include <cstdlib>
 #include <random>
@@ -314,6 +315,52 @@ static void idd_pipeline_tests()
     std::puts("PASS incoherent_dedispersion_pipeline");
 }
 
+// ObservationHeader.cpp:6-33 + MultiFileReader.cu + MultiFileWriter.cu
+static void dada_io_tests(const std::string& scratch)
+{
+    const std::string hdr_text =
+        "HEADER DADA\nHDR_SIZE 4096\nNCHAN 64\nOBS_NCHAN 4096\nNPOL 2\nNBIT 8\nNANT 57\n"
+        "SAMPLE_CLOCK_START 0\nBW 13375000.0\nOBS_BW 856000000.0\nFREQ 1284000000.0\n"
+        "OBS_FREQ 1284000000.0\nTSAMP 4.785\nSAMPLE_CLOCK 1712000000.0\nSYNC_TIME 0\n"
+        "UTC_START 1708082229.0\nMJD_START 60356.47\nSOURCE J1644-4559\nRA 16:44:49.27\n"
+        "DEC -45:59:09.7\nTELESCOPE MeerKAT\nINSTRUMENT CBF-Feng\nCHAN0_IDX 2688\n";
+    std::vector<int8_t> payload = normal_int8(10000, 20.0f, 9);
+    std::vector<std::string> files;
+    for(int i = 0; i < 2; ++i) {
+        std::string h = hdr_text + "OBS_OFFSET " + std::to_string(i * 6000) + "\n";
+        h.resize(4096, '\0');
+        files.push_back(scratch + "/in" + std::to_string(i) + ".dada");
+        std::ofstream f(files.back(), std::ios::binary);
+        f.write(h.data(), (std::streamsize)h.size());
+        f.write(reinterpret_cast<const char*>(payload.data()) + i * 6000, i ? 4000 : 6000);
+    }
+    MultiFileReader r(files, 4096, true);
+    EXPECT(r.get_total_size() == 10000);
+    EXPECT(r.get_header().nantennas == 57 && r.get_header().chan0_idx == 2688);
+    std::vector<int8_t> back(10000);
+    EXPECT(r.read(reinterpret_cast<char*>(back.data()), 10000) == 10000);
+    EXPECT(back == payload && r.eof());
+    {
+        MultiFileWriter w(scratch + "/out", r.get_header(), 5000, "I", "sw", "cb");
+        MultiFileWriter::StreamInfo s{32, 64, 40, 0, {}, 150.0f, 1.9e-5, 0.0, "TFB"};
+        for(int k = 0; k < 3; ++k) w(payload.data() + k * 2560, 2560, s, 1);
+    }
+    const std::string dir = scratch + "/out/2024-02-16-11:17:09/1/1284000000/";
+    const std::string base = dir + "sw_2024-02-16-11:17:09_1_00150.000_1284000000_cb_";
+    std::ifstream f0(base + "0000000000000000.tfb", std::ios::binary);
+    EXPECT(f0.good());
+    std::string h0(4096, '\0');
+    f0.read(&h0[0], 4096);
+    char v[64];
+    EXPECT(sw_dada_header_get(h0.data(), 4096, "NBEAM", v, sizeof(v)) == SW_OK && std::string(v) == "32");
+    EXPECT(sw_dada_header_get(h0.data(), 4096, "ORDER", v, sizeof(v)) == SW_OK && std::string(v) == "TFB");
+    EXPECT(sw_dada_header_get(h0.data(), 4096, "FILE_SIZE", v, sizeof(v)) == SW_OK && std::string(v) == "2560");
+    // 5000-byte limit rounded down to whole 2560-byte blocks: three files
+    std::ifstream f1(base + "0000000000002560.tfb", std::ios::binary), f2(base + "0000000000005120.tfb", std::ios::binary);
+    EXPECT(f1.good() && f2.good());
+    std::puts("PASS dada_io");
+}
+
 int main(int argc, char** argv)
 {
     const std::string golden = argc > 1 ? argv[1] : "tests/golden";
@@ -326,6 +373,7 @@ int main(int argc, char** argv)
     dedispersion_plan_tests();
     pipeline_smoke(golden);
     idd_pipeline_tests();
+    dada_io_tests(argc > 2 ? argv[2] : ".");
     std::puts("ALL PASS");
     return 0;
 }

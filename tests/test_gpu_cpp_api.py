@@ -28,7 +28,10 @@ def _build(oracle):
 
 def test_cpp_stage_api(cuda, oracle):
     exe = _build(oracle)
-    r = subprocess.run([exe, GOLDEN], capture_output=True, text=True, timeout=300)
+    scratch = os.path.join(REPO, "skyweaver_b200", "_build", "cpp_scratch")
+    shutil.rmtree(scratch, ignore_errors=True)
+    os.makedirs(scratch)
+    r = subprocess.run([exe, GOLDEN, scratch], capture_output=True, text=True, timeout=300)
     print(r.stdout)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "ALL PASS" in r.stdout

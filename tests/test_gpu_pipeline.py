@@ -8,6 +8,7 @@ by one LSB against the FP64 oracle, which can move a beam sample by one LSB:
 those are bounded in count below.
 """
 import math
+import os
 
 import numpy as np
 import pytest
@@ -357,3 +358,75 @@ def test_uhf_pipeline_with_incoherent_dedispersion_vs_oracle(cuda, oracle):
     print("DM 300 block S/N per trial: gpu", np.round(gpu, 1), "cpu", np.round(cpu, 1))
     assert best == int(np.argmin(np.abs(trials[1] - 300.0)))
     assert gpu[best] > 8 and abs(gpu[best] - cpu[best]) < 0.05 * cpu[best]
+
+
+def test_dada_files_through_pipeline_to_dada_outputs(cuda, tmp_path):
+    """DADA ingest -> pipeline -> DADA output: TAFTP gulps read from two
+    contiguous DADA files by the pinned double-buffered gulp reader, run
+    through the host API, and each coherent DM's beams written as size-split
+    DADA streams; the written payload equals the beams of the same gulps run
+    from device memory."""
+    torch = cuda
+    from skyweaver_b200 import dada, stages, synthetic
+    from test_dada_io import _header
+    g = synthetic.rng(5150)
+    A, F, B, T, ts = 32, 4, 64, 4096, 16
+    chbw = 856e6 / 1024
+    centre, bw = 1284e6, F * chbw
+    dms = [0.0, 30.0]
+    ngulps = 3
+    gulps = [synthetic.voltages_taftp(g, T // 256, A, F, sigma=8) for _ in range(ngulps)]
+    payload = np.concatenate([x.reshape(-1) for x in gulps])
+    cut = payload.size // 2 + 123
+    files = []
+    for i, (a, b) in enumerate(((0, cut), (cut, payload.size))):
+        p = tmp_path / f"in{i}.dada"
+        p.write_bytes(_header(a, NCHAN=str(F), NANT=str(A)) + payload[a:b].tobytes())
+        files.append(str(p))
+    delays = synthetic.delay_model(g, B, A)
+    kw = dict(nantennas=A, input_nantennas=A, nchans=F, nbeams=B, gulp_samples=T, tscrunch=ts,
+              centre_frequency=centre, bandwidth=bw, dms=dms, beamset_weights=np.ones((1, A)),
+              beamset_mapping=np.zeros(B, np.int32))
+    # reference: the same gulps from device memory
+    ref = [[] for _ in dms]
+    pipe = stages.BeamformerPipeline(**kw)
+    pipe.set_delays(delays, 1.7e9)
+    for i, x in enumerate(gulps):
+        pipe.process_device(torch.from_numpy(x).cuda(), 1.7e9 + i * T / chbw)
+        for d in range(len(dms)):
+            ref[d].append(pipe.outputs(d)["cb"])
+    pipe.close()
+    # DADA in -> host API -> DADA out
+    reader = dada.MultiFileReader(files, check_contiguity=True)
+    hdr = reader.header().as_dict()
+    dada.validate_header(reader.header(), A, F, 2)
+    pipe = stages.BeamformerPipeline(**kw)
+    pipe.set_delays(delays, 1.7e9)
+    per_dm = pipe.cb_bytes_per_dm()
+    out = torch.empty(per_dm * len(dms), dtype=torch.int8, pin_memory=True)
+    writers = []
+    for d, dm in enumerate(dms):
+        dr, base, ext = dada.output_paths(str(tmp_path / "out"), hdr, d, dm, "TFB")
+        w = dada.FileStream(dr, base, ext, 2 * per_dm)
+        w.set("NBEAM", B)
+        w.set("COHERENT_DM", dm)
+        writers.append((w, dr))
+    gr = dada.GulpReader(reader, payload.size // ngulps)
+    n = 0
+    for buf, i in gr:
+        pipe.process_host(buf, 1.7e9 + i * T / chbw, out)
+        torch.cuda.synchronize()
+        host = out.numpy()
+        for d, (w, _) in enumerate(writers):
+            w.write(host[d * per_dm:(d + 1) * per_dm])
+        n += 1
+    gr.close()
+    reader.close()
+    pipe.close()
+    assert n == ngulps
+    for d, (w, dr) in enumerate(writers):
+        w.close()
+        names = sorted(os.listdir(dr))
+        assert len(names) == 2                       # 3 gulps in files of 2 gulps
+        data = b"".join(open(os.path.join(dr, nm), "rb").read()[4096:] for nm in names)
+        assert data == np.concatenate([r.reshape(-1) for r in ref[d]]).tobytes()
