@@ -93,3 +93,52 @@ def test_reference_arm_nonzero_rank_does_no_work():
                        capture_output=True, text=True, timeout=120, env=env)
     assert r.returncode == 0, r.stderr
     assert r.stdout.strip() == ""
+
+
+def _exchange_main(rank, world, port, out_dir):
+    import torch
+    import torch.distributed as dist
+    sys.path.insert(0, REPO)
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    from skyweaver_b200 import subbands
+    import swb_oracle as oracle
+    oracle.build()
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
+                            world_size=world)
+    try:
+        T, F, B = 600, 16, 24
+        full = np.random.default_rng(7).integers(-128, 128, size=(T, F, B), dtype=np.int8)
+        mine = torch.from_numpy(np.ascontiguousarray(full[:, subbands.rank_channels(F, world, rank)]))
+        got = subbands.channels_to_beams(mine).numpy()
+        np.save(os.path.join(out_dir, f"beams{rank}.npy"), got)
+        # incoherent dedispersion of this rank's beams over the whole band
+        freqs = 1284e6 + (np.arange(F) - F / 2) * 0.8359375e6
+        delays, maxd = oracle.idd_delays(freqs, np.array([0, 40, 80], np.float32), 1.9e-5)
+        n = T - (T - maxd) % 2
+        tdb = oracle.idd(np.ascontiguousarray(got[:n]), delays, maxd, 2, np.float32(4.0))
+        np.save(os.path.join(out_dir, f"tdb{rank}.npy"), tdb)
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_channel_partition_exchange_to_beam_blocks(tmp_path, oracle):
+    """Channel-partitioned ranks + one all-to-all give each rank every
+    channel of its beam block, and the incoherent dedispersion of those
+    blocks equals that of the single-process array."""
+    import torch.multiprocessing as mp
+    world = 2
+    mp.start_processes(_exchange_main, args=(world, _free_port(), str(tmp_path)), nprocs=world,
+                       join=True, start_method="spawn")
+    sys.path.insert(0, REPO)
+    from skyweaver_b200 import subbands
+    T, F, B = 600, 16, 24
+    full = np.random.default_rng(7).integers(-128, 128, size=(T, F, B), dtype=np.int8)
+    freqs = 1284e6 + (np.arange(F) - F / 2) * 0.8359375e6
+    delays, maxd = oracle.idd_delays(freqs, np.array([0, 40, 80], np.float32), 1.9e-5)
+    n = T - (T - maxd) % 2
+    ref = oracle.idd(np.ascontiguousarray(full[:n]), delays, maxd, 2, np.float32(4.0))
+    for r in range(world):
+        bs = subbands.rank_beams(B, world, r)
+        assert np.array_equal(np.load(tmp_path / f"beams{r}.npy"), full[:, :, bs])
+        assert np.array_equal(np.load(tmp_path / f"tdb{r}.npy"), ref[:, :, bs])
