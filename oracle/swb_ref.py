@@ -1,0 +1,102 @@
+"""ctypes access to oracle/_ref/libswref.so: the reference's own stage
+implementations built from its sources (oracle/Makefile, target `ref`; see
+ref_driver.cu).  Test infrastructure only: the GPU parity tests use it to
+pin the oracle restatement and the B200 kernels to the reference itself.
+Shapes are the build's compile-time constants (shape())."""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_ref", "libswref.so")
+_lib = None
+
+
+def available() -> bool:
+    return os.path.exists(LIB)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = ctypes.CDLL(LIB)
+        _lib.swref_error.restype = ctypes.c_char_p
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _check(rc):
+    if rc != 0:
+        raise RuntimeError(lib().swref_error().decode())
+
+
+def shape():
+    v = [ctypes.c_int() for _ in range(5)]
+    lib().swref_shape(*[ctypes.byref(x) for x in v])
+    return dict(zip(("nant", "nchans", "nbeams", "cb_ts", "ib_ts"), (x.value for x in v)))
+
+
+def transpose(taftp, input_nant):
+    s = shape()
+    H = taftp.shape[0]
+    out = np.empty((s["nchans"], H * 256, 2, s["nant"], 2), np.int8)
+    _check(lib().swref_transpose(_p(np.ascontiguousarray(taftp)), H, input_nant, _p(out)))
+    return out
+
+
+def statistics(ftpa):
+    s = shape()
+    T = ftpa.shape[1]
+    out = np.empty((s["nchans"], 2, s["nant"], 4), np.float32)
+    _check(lib().swref_statistics(_p(np.ascontiguousarray(ftpa)), T, _p(out)))
+    return out
+
+
+def beamform(ftpa, weights, cb_scale, cb_offset, ib_scale, ib_offset, beamset_weights, mapping):
+    s = shape()
+    F, T, B = s["nchans"], ftpa.shape[1], s["nbeams"]
+    S = beamset_weights.shape[0]
+    ts = s["cb_ts"]
+    raw = np.empty((S, T // ts, F), np.float32)
+    ib = np.empty((S, T // ts, F), np.int8)
+    cb = np.empty((T // ts, F, B), np.int8)
+    f32 = lambda a: np.ascontiguousarray(a, np.float32)
+    _check(lib().swref_beamform(_p(np.ascontiguousarray(ftpa)), T, _p(np.ascontiguousarray(weights)),
+                                _p(f32(cb_scale)), _p(f32(cb_offset)), _p(f32(ib_scale)),
+                                _p(f32(ib_offset)), _p(f32(beamset_weights)),
+                                _p(np.ascontiguousarray(mapping, np.int32)), S, _p(raw), _p(ib),
+                                _p(cb)))
+    return raw, ib, cb
+
+
+def weights(delays, current_epoch, delay_epoch, centre, bw):
+    s = shape()
+    out = np.empty((s["nchans"], s["nbeams"], s["nant"], 2), np.int8)
+    lib().swref_weights.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double,
+                                    ctypes.c_double, ctypes.c_double, ctypes.c_void_p]
+    _check(lib().swref_weights(_p(np.ascontiguousarray(delays, np.float32)), current_epoch,
+                               delay_epoch, centre, bw, _p(out)))
+    return out
+
+
+def idd(tfb, dms, tscrunch, centre, bw):
+    s = shape()
+    T = tfb.shape[0]
+    dms = np.ascontiguousarray(dms, np.float32)
+    delays = np.empty((len(dms), s["nchans"]), np.int32)
+    maxd = ctypes.c_int()
+    lib().swref_idd.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
+                                ctypes.c_void_p, ctypes.c_void_p]
+    # TDB rows: (T - max_delay) / tscrunch; allocate for the largest case
+    out = np.empty((T // tscrunch + 1) * len(dms) * s["nbeams"], np.int8)
+    _check(lib().swref_idd(_p(np.ascontiguousarray(tfb)), T, _p(dms), len(dms), tscrunch, centre,
+                           bw, _p(out), _p(delays), ctypes.byref(maxd)))
+    n = (T - maxd.value) // tscrunch
+    return out[:n * len(dms) * s["nbeams"]].reshape(n, len(dms), s["nbeams"]), delays, maxd.value

@@ -1,0 +1,119 @@
+"""Pin the oracle, and the B200 kernels, to the reference implementation
+itself: the reference's own stage classes (Transposer, StatisticsCalculator,
+WeightsManager, IncoherentBeamformer, CoherentBeamformer,
+IncoherentDedisperser) built from its sources into oracle/_ref/libswref.so
+(oracle/Makefile `ref`), at that build's compile-time shape (64 antennas,
+16 channels, 128 beams, tscrunch 16).
+
+Tolerances are the reference's own GPU-vs-CPU test tolerances: exact for the
+transpose, weights and incoherent dedispersion (TransposerTester.cu:90-91,
+WeightsManagerTester.cu:94-95, a host implementation), 1e-5 relative for the
+statistics (StatisticsCalculatorTester.cu:152-170), +-1 for the int8 beams
+(CoherentBeamformerTester.cu:43, its GPU kernel contracts the float chain
+into FMAs).  The oracle and the B200 kernels follow the reference's CPU
+implementations and agree with each other bit for bit."""
+import math
+import sys
+
+import numpy as np
+import pytest
+
+from conftest import REPO
+
+sys.path.insert(0, REPO + "/oracle")
+import swb_ref  # noqa: E402
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not swb_ref.available(),
+                                 reason="oracle/_ref not built (needs the reference sources)")]
+
+CENTRE, CHBW = 1284e6, 856e6 / 1024
+
+
+def _dev(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def test_transpose_matches_reference(cuda, oracle):
+    from skyweaver_b200 import stages, synthetic
+    s = swb_ref.shape()
+    taftp = synthetic.voltages_taftp(synthetic.rng(1), 8, 57, s["nchans"], sigma=30)
+    ref = swb_ref.transpose(taftp, 57)
+    assert np.array_equal(oracle.transpose(taftp, s["nant"]), ref)
+    got = stages.transpose_ftpa(_dev(cuda, taftp), s["nant"]).cpu().numpy()
+    assert np.array_equal(got, ref)
+
+
+def test_statistics_and_weights_match_reference(cuda, oracle):
+    from skyweaver_b200 import stages, synthetic
+    s = swb_ref.shape()
+    g = synthetic.rng(2)
+    ftpa = oracle.transpose(synthetic.voltages_taftp(g, 16, s["nant"], s["nchans"]), s["nant"])
+    ref = swb_ref.statistics(ftpa)
+    np.testing.assert_allclose(oracle.statistics(ftpa), ref, rtol=1e-5, atol=1e-5)
+    bw = s["nchans"] * CHBW
+    freqs = stages.channel_frequencies(CENTRE, bw, s["nchans"])
+    delays = synthetic.delay_model(g, s["nbeams"], s["nant"])
+    wref = swb_ref.weights(delays, 10.0, 9.0, CENTRE, bw)
+    assert np.array_equal(oracle.weights(delays, freqs, 10.0, 9.0), wref)
+    fba, _ = stages.generate_weights(_dev(cuda, delays), _dev(cuda, freqs), 10.0, 9.0)
+    assert np.array_equal(fba.cpu().numpy(), wref)
+
+
+def test_beamformers_match_reference(cuda, oracle):
+    from skyweaver_b200 import stages, synthetic
+    s = swb_ref.shape()
+    A, F, B, ts = s["nant"], s["nchans"], s["nbeams"], s["cb_ts"]
+    g = synthetic.rng(3)
+    T = 8192                                   # the reference CB needs T/ts % 512 == 0
+    taftp = synthetic.voltages_taftp(g, T // 256, A, F, sigma=32)
+    ftpa = oracle.transpose(taftp, A)
+    th = g.uniform(0, 2 * np.pi, size=(F, B, A))
+    w = np.stack([np.rint(127 * np.cos(th)), np.rint(127 * np.sin(th))], -1).astype(np.int8)
+    level = 32.0
+    cb_s = (127 * level * math.sqrt(A)) ** 2
+    dof = 2 * ts * 2
+    cb_scale = np.full(F, cb_s * math.sqrt(2 * dof) / level, np.float32)
+    cb_off = np.full(F, cb_s * dof, np.float32)
+    ib_dof = 2 * ts * A * 2
+    ib_scale = np.full(F, level ** 2 * math.sqrt(2 * ib_dof) / level, np.float32)
+    ib_off = np.full(F, level ** 2 * ib_dof, np.float32)
+    bw1 = np.ones((1, A), np.float32)
+    mapping = np.zeros(B, np.int32)
+    raw_r, ib_r, cb_r = swb_ref.beamform(ftpa, w, cb_scale, cb_off, ib_scale, ib_off, bw1,
+                                         mapping)
+    raw_o, ib_o = oracle.incoherent_beam(ftpa, ts, ib_scale, ib_off, bw1, 1)
+    cb_o = oracle.coherent_beam(ftpa, w, ts, cb_scale, cb_off, bw1, mapping)
+    np.testing.assert_allclose(raw_o, raw_r, rtol=1e-6)
+    assert np.abs(ib_o.astype(int) - ib_r.astype(int)).max() <= 1
+    d = np.abs(cb_o.astype(int) - cb_r.astype(int))
+    print(f"CB oracle vs reference GPU kernel: {(d > 0).mean():.2e} of samples differ, max {d.max()}")
+    assert d.max() <= 1 and (d > 0).mean() < 1e-2
+    # the B200 kernels equal the oracle exactly
+    fp = stages.transpose_fpact(_dev(cuda, taftp), A)
+    raw_g, ib_g = stages.incoherent_beamform(fp, T, ts, _dev(cuda, ib_scale), _dev(cuda, ib_off),
+                                             _dev(cuda, bw1))
+    cb_g = stages.coherent_beamform(fp, stages.pack_weights(_dev(cuda, w)), _dev(cuda, cb_scale),
+                                    _dev(cuda, cb_off), _dev(cuda, mapping), raw_g, T, ts)
+    assert np.array_equal(raw_g.cpu().numpy(), raw_o)
+    assert np.array_equal(cb_g.cpu().numpy(), cb_o)
+
+
+def test_incoherent_dedisperser_matches_reference(cuda, oracle):
+    from skyweaver_b200 import stages, synthetic
+    s = swb_ref.shape()
+    F, B = s["nchans"], s["nbeams"]
+    bw = F * CHBW
+    dms = np.array([0.0, 100.0, 300.0, 500.0], np.float32)
+    for ts in (1, 4):
+        g = synthetic.rng(4 + ts)
+        freqs = stages.channel_frequencies(CENTRE, bw, F)
+        delays, maxd = oracle.idd_delays(freqs, dms, s["cb_ts"] / CHBW)
+        T = maxd + 64 * ts
+        tfb = g.integers(-128, 128, size=(T, F, B), dtype=np.int8)
+        ref, dref, mref = swb_ref.idd(tfb, dms, ts, CENTRE, bw)
+        assert mref == maxd and np.array_equal(dref, delays)
+        sf = np.float32(math.sqrt(F * ts))
+        assert np.array_equal(oracle.idd(tfb, delays, maxd, ts, sf), ref)
+        got = stages.incoherent_dedisperse(_dev(cuda, tfb), _dev(cuda, delays), maxd, ts, float(sf))
+        assert np.array_equal(got.cpu().numpy(), ref)
