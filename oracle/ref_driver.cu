@@ -134,6 +134,49 @@ int swref_beamform(const int8_t* ftpa, int nsamples, const int8_t* weights, cons
     });
 }
 
+// Device time of one IncoherentBeamformer and one CoherentBeamformer
+// beamform call on nsamples of synthetic device data (mean over reps after a
+// warm-up; the calls synchronise their stream, as in the reference).
+int swref_time_beamform(int nsamples, int reps, float* ms_ib, float* ms_cb)
+{
+    return guarded([&] {
+        PipelineConfig& c = config(1284e6, 13.375e6);
+        const std::size_t F = c.nchans(), A = c.nantennas(), B = c.nbeams();
+        FTPAVoltagesH<char2> h({F, (std::size_t)nsamples, c.npol(), A});
+        for(std::size_t i = 0; i < h.size(); ++i)
+            h[i] = make_char2((signed char)((i * 2654435761u >> 13) % 31 - 15),
+                              (signed char)((i * 40503u >> 7) % 31 - 15));
+        FTPAVoltagesD<char2> d = h;
+        thrust::device_vector<char2> wd(F * B * A, make_char2(90, -90));
+        thrust::device_vector<float> sc(F, 1e9f), of(F, 0.0f), bw(A, 1.0f);
+        thrust::device_vector<int> map(B, 0);
+        IncoherentBeamformer<Traits> ib(c);
+        CoherentBeamformer<Traits> cb(c);
+        typename IncoherentBeamformer<Traits>::RawPowerVectorTypeD raw;
+        typename IncoherentBeamformer<Traits>::PowerVectorTypeD ibq;
+        typename CoherentBeamformer<Traits>::PowerVectorTypeD tfb;
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        ib.beamform(d, raw, ibq, sc, of, bw, 1, 0);
+        cudaEventRecord(e0, 0);
+        for(int r = 0; r < reps; ++r) ib.beamform(d, raw, ibq, sc, of, bw, 1, 0);
+        cudaEventRecord(e1, 0);
+        cudaEventSynchronize(e1);
+        cudaEventElapsedTime(ms_ib, e0, e1);
+        *ms_ib /= reps;
+        cb.beamform(d, wd, sc, of, map, raw, tfb, 1, 0);
+        cudaEventRecord(e0, 0);
+        for(int r = 0; r < reps; ++r) cb.beamform(d, wd, sc, of, map, raw, tfb, 1, 0);
+        cudaEventRecord(e1, 0);
+        cudaEventSynchronize(e1);
+        cudaEventElapsedTime(ms_cb, e0, e1);
+        *ms_cb /= reps;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    });
+}
+
 // delays float3 [NBEAMS][NANT] -> weights FBA char2 [F][NBEAMS][NANT]
 int swref_weights(const float* delays, double current_epoch, double delay_epoch, double centre,
                   double bw, int8_t* weights)

@@ -100,3 +100,18 @@ def idd(tfb, dms, tscrunch, centre, bw):
                            bw, _p(out), _p(delays), ctypes.byref(maxd)))
     n = (T - maxd.value) // tscrunch
     return out[:n * len(dms) * s["nbeams"]].reshape(n, len(dms), s["nbeams"]), delays, maxd.value
+
+
+LIB_C1 = os.path.join(HERE, "_ref", "c1", "libswref_c1.so")
+
+
+def time_beamform_c1(nsamples=65536, reps=3):
+    """Device ms of the reference's own IncoherentBeamformer and
+    CoherentBeamformer (Stokes I) at 64 antennas x 64 channels x 1024 beams,
+    tscrunch 16, one call each (oracle/_ref/c1)."""
+    lc = ctypes.CDLL(LIB_C1)
+    lc.swref_error.restype = ctypes.c_char_p
+    ib, cb = ctypes.c_float(), ctypes.c_float()
+    if lc.swref_time_beamform(nsamples, reps, ctypes.byref(ib), ctypes.byref(cb)) != 0:
+        raise RuntimeError(lc.swref_error().decode())
+    return ib.value, cb.value

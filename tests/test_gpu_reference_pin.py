@@ -117,3 +117,43 @@ def test_incoherent_dedisperser_matches_reference(cuda, oracle):
         assert np.array_equal(oracle.idd(tfb, delays, maxd, ts, sf), ref)
         got = stages.incoherent_dedisperse(_dev(cuda, tfb), _dev(cuda, delays), maxd, ts, float(sf))
         assert np.array_equal(got.cpu().numpy(), ref)
+
+
+@pytest.mark.skipif(not __import__("os").path.exists(swb_ref.LIB_C1),
+                    reason="oracle/_ref/c1 not built")
+def test_reference_gpu_beamformer_timing(cuda):
+    """The reference's own GPU beamformers (dp4a CUDA-core kernels built for
+    sm_100a at the benchmark shape: 64 antennas, 64 channels, 1024 beams,
+    tscrunch 16, one DM of 65536 samples) timed beside ours on the same
+    B200; ours must be faster."""
+    torch = cuda
+    from skyweaver_b200 import stages
+    ms_ib_ref, ms_cb_ref = swb_ref.time_beamform_c1()
+    A, F, B, T, ts = 64, 64, 1024, 65536, 16
+    gen = torch.Generator(device="cuda").manual_seed(3)
+    fp = (torch.randn((F, 2, A, 2, T), generator=gen, device="cuda") * 8).round_().clamp_(-127, 127)
+    fp = fp.to(torch.int8)
+    gemm = torch.randint(-127, 128, (F, 2, B, A, 2), dtype=torch.int8, device="cuda")
+    sc = torch.full((F,), 1e9, device="cuda")
+    bw = torch.ones((1, A), device="cuda")
+    mapping = torch.zeros(B, dtype=torch.int32, device="cuda")
+    raw, _ = stages.incoherent_beamform(fp, T, ts, sc, sc, bw)
+
+    def timeit(fn, reps=5):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    ms_ib = timeit(lambda: stages.incoherent_beamform(fp, T, ts, sc, sc, bw))
+    ms_cb = timeit(lambda: stages.coherent_beamform(fp, gemm, sc, sc, mapping, raw, T, ts))
+    ops = 8.0 * A * B * 2 * F * T
+    print(f"reference GPU: IB {ms_ib_ref:.3f} ms, CB {ms_cb_ref:.3f} ms "
+          f"({ops / ms_cb_ref / 1e9:.0f} TOPS); "
+          f"B200 kernels: IB {ms_ib:.3f} ms, CB {ms_cb:.3f} ms ({ops / ms_cb / 1e9:.0f} TOPS)")
+    assert ms_cb < ms_cb_ref and ms_ib < ms_ib_ref
