@@ -10,13 +10,16 @@
 // StatisticsCalculator::calculate_statistics (src/StatisticsCalculator.cu:
 // 104-130), IncoherentBeamformer / CoherentBeamformer<Stokes I>::beamform
 // (src/IncoherentBeamformer.cu:108-182, src/CoherentBeamformer.cu:191-270),
-// WeightsManager::weights (src/WeightsManager.cu:109-139) and
-// IncoherentDedisperser::dedisperse (src/IncoherentDedisperser.cu:66-125).
+// WeightsManager::weights (src/WeightsManager.cu:109-139),
+// IncoherentDedisperser::dedisperse (src/IncoherentDedisperser.cu:66-125) and
+// CoherentDedisperser::dedisperse (src/CoherentDedisperser.cu:142-225, timed
+// only).
 #include <cstring>
 #include <stdexcept>
 #include <vector>
 
 #include "skyweaver/CoherentBeamformer.cuh"
+#include "skyweaver/CoherentDedisperser.cuh"
 #include "skyweaver/DescribedVector.hpp"
 #include "skyweaver/IncoherentBeamformer.cuh"
 #include "skyweaver/IncoherentDedisperser.cuh"
@@ -172,6 +175,45 @@ int swref_time_beamform(int nsamples, int reps, float* ms_ib, float* ms_cb)
         cudaEventSynchronize(e1);
         cudaEventElapsedTime(ms_cb, e0, e1);
         *ms_cb /= reps;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    });
+}
+
+// Device time of the reference's coherent dedispersion of one gulp: one
+// CoherentDedisperser::dedisperse call (int8 -> complex, batched cuFFT
+// forward, chirp, cuFFT inverse, trim, requantise) per (channel, DM), as its
+// pipeline issues them (detail/BeamformerPipeline.cu:192-205).
+int swref_time_cdd(int fft_length, int overlap, const float* dms, int ndms, double centre,
+                   double bw, int reps, float* ms)
+{
+    return guarded([&] {
+        PipelineConfig& c = config(centre, bw);
+        CoherentDedisperserConfig cfg;
+        create_coherent_dedisperser_config(cfg, fft_length, overlap, c.nchans(), c.npol(),
+                                           c.nantennas(), c.nchans() / bw, centre - bw / 2, bw,
+                                           std::vector<float>(dms, dms + ndms));
+        CoherentDedisperser cd(cfg);
+        TPAVoltagesH<char2> h({(std::size_t)fft_length, c.npol(), c.nantennas()});
+        for(std::size_t i = 0; i < h.size(); ++i)
+            h[i] = make_char2((signed char)((i * 2654435761u >> 13) % 31 - 15),
+                              (signed char)((i * 40503u >> 7) % 31 - 15));
+        TPAVoltagesD<char2> in = h;
+        FTPAVoltagesD<char2> out({c.nchans(), (std::size_t)(fft_length - overlap), c.npol(),
+                                  c.nantennas()});
+        cd.dedisperse(in, out, 0, 0);
+        cudaDeviceSynchronize();
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0, 0);
+        for(int r = 0; r < reps; ++r)
+            for(unsigned f = 0; f < c.nchans(); ++f)
+                for(int d = 0; d < ndms; ++d) cd.dedisperse(in, out, f, d);
+        cudaEventRecord(e1, 0);
+        cudaEventSynchronize(e1);
+        cudaEventElapsedTime(ms, e0, e1);
+        *ms /= reps;
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
     });

@@ -115,3 +115,20 @@ def time_beamform_c1(nsamples=65536, reps=3):
     if lc.swref_time_beamform(nsamples, reps, ctypes.byref(ib), ctypes.byref(cb)) != 0:
         raise RuntimeError(lc.swref_error().decode())
     return ib.value, cb.value
+
+
+def time_cdd_c1(dms, fft_length=65536, overlap=1472, centre=1284e6, bw=64 * 856e6 / 1024,
+                reps=2):
+    """Device ms per gulp of the reference's own coherent dedispersion: one
+    CoherentDedisperser::dedisperse call per (channel, DM) at 64 channels x
+    2 pols x 64 antennas (oracle/_ref/c1)."""
+    lc = ctypes.CDLL(LIB_C1)
+    lc.swref_error.restype = ctypes.c_char_p
+    lc.swref_time_cdd.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                  ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_void_p]
+    d = np.ascontiguousarray(dms, np.float32)
+    ms = ctypes.c_float()
+    if lc.swref_time_cdd(fft_length, overlap, _p(d), len(d), centre, bw, reps,
+                         ctypes.byref(ms)) != 0:
+        raise RuntimeError(lc.swref_error().decode())
+    return ms.value

@@ -157,3 +157,34 @@ def test_reference_gpu_beamformer_timing(cuda):
           f"({ops / ms_cb_ref / 1e9:.0f} TOPS); "
           f"B200 kernels: IB {ms_ib:.3f} ms, CB {ms_cb:.3f} ms ({ops / ms_cb / 1e9:.0f} TOPS)")
     assert ms_cb < ms_cb_ref and ms_ib < ms_ib_ref
+
+
+@pytest.mark.skipif(not __import__("os").path.exists(swb_ref.LIB_C1),
+                    reason="oracle/_ref/c1 not built")
+def test_reference_gpu_dedisperser_timing(cuda):
+    """The reference's own coherent dedispersion (cuFFT, one call per
+    channel and DM, 65536-point windows) for a gulp of 64 channels x 2 pols x
+    64 antennas at DMs {0, 50, 150, 500}, timed beside ours on the same B200;
+    ours must be faster."""
+    torch = cuda
+    from skyweaver_b200 import stages
+    dms = [0.0, 50.0, 150.0, 500.0]
+    ms_ref = swb_ref.time_cdd_c1(dms)
+    F, A, T, ov = 64, 64, 65536, 1472
+    bw = F * CHBW
+    low = float(np.float32(CENTRE - bw / 2))
+    cdd = stages.CoherentDedisperser(F, A, 8192, ov, low, bw, dms)
+    ext = torch.randint(-40, 40, (F, 2, A, 2, ov + T), dtype=torch.int8, device="cuda")
+    outs = [torch.empty((F, 2, A, 2, T), dtype=torch.int8, device="cuda") for _ in dms]
+    cdd.dedisperse(ext, T, outs)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(3):
+        cdd.dedisperse(ext, T, outs)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / 3
+    print(f"reference GPU coherent dedispersion: {ms_ref:.1f} ms per gulp; "
+          f"B200 kernel: {ms:.2f} ms per gulp ({ms_ref / ms:.1f}x)")
+    assert ms < ms_ref
