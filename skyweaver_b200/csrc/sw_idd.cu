@@ -75,10 +75,11 @@ idd_k(const uint32_t* __restrict__ tfb, int nchans, int nquads,
     tdb[((size_t)to * ndms + d) * nquads + q] = packed;
 }
 
-// Same sums, four beam quads (16 beams, one 16-byte load) per thread: the
-// per-load address work is shared by 16 beams and each channel's row offset
-// comes from a per-CTA table in shared memory.  Needs nbeams % 16 == 0 and
-// 16-byte aligned buffers.  Block order as idd_k.
+// Same sums, 16 * V beams per thread (V 16-byte loads from one row): the
+// per-load address work is shared by many beams and each channel's row offset
+// comes from a per-CTA table in shared memory.  Needs nbeams % (16 V) == 0
+// and 16-byte aligned buffers.  Block order as idd_k.
+template <int V>
 __global__ void __launch_bounds__(128)
 idd16_k(const uint4* __restrict__ tfb, int nchans, int nq16,
         const int* __restrict__ delays, int max_delay, int tscrunch,
@@ -99,30 +100,36 @@ idd16_k(const uint4* __restrict__ tfb, int nchans, int nq16,
     for(int f = threadIdx.x; f < nchans; f += blockDim.x)
         s_off[f] = (long long)f * nq16 - (long long)dl_f[f] * row;
     __syncthreads();
-    const int q = qb * blockDim.x + threadIdx.x;
+    const int q = (qb * blockDim.x + threadIdx.x) * V;  // first uint4 of this thread
     if(q >= nq16) return;
     const int t = max_delay + to * tscrunch;
-    int acc[16];
+    int acc[16 * V];
 #pragma unroll
-    for(int k = 0; k < 16; ++k) acc[k] = 0;
+    for(int k = 0; k < 16 * V; ++k) acc[k] = 0;
     for(int tau = 0; tau < tscrunch; ++tau) {
         const uint4* bt = tfb + (long long)(t + tau) * row + q;
         for(int f0 = 0; f0 < nchans; f0 += 256) {
             const int f1 = min(nchans, f0 + 256);
-            uint32_t lo[4] = {0, 0, 0, 0}, hi[4] = {0, 0, 0, 0};
+            uint32_t lo[4 * V], hi[4 * V];
+#pragma unroll
+            for(int k = 0; k < 4 * V; ++k) lo[k] = hi[k] = 0;
 #pragma unroll 4
             for(int f = f0; f < f1; ++f) {
-                const uint4 v = bt[s_off[f]];
-                const uint32_t w[4] = {v.x ^ 0x80808080u, v.y ^ 0x80808080u,
-                                       v.z ^ 0x80808080u, v.w ^ 0x80808080u};
+                const uint4* p = bt + s_off[f];
 #pragma unroll
-                for(int k = 0; k < 4; ++k) {
-                    lo[k] += prmt(w[k], 0, 0x4240);  // bytes 0,2 -> 16-bit lanes
-                    hi[k] += prmt(w[k], 0, 0x4341);  // bytes 1,3
+                for(int u = 0; u < V; ++u) {
+                    const uint4 v = p[u];
+                    const uint32_t w[4] = {v.x ^ 0x80808080u, v.y ^ 0x80808080u,
+                                           v.z ^ 0x80808080u, v.w ^ 0x80808080u};
+#pragma unroll
+                    for(int k = 0; k < 4; ++k) {
+                        lo[4 * u + k] += prmt(w[k], 0, 0x4240);  // bytes 0,2 -> 16-bit lanes
+                        hi[4 * u + k] += prmt(w[k], 0, 0x4341);  // bytes 1,3
+                    }
                 }
             }
 #pragma unroll
-            for(int k = 0; k < 4; ++k) {  // at most 256 adds of <= 255 per lane
+            for(int k = 0; k < 4 * V; ++k) {  // at most 256 adds of <= 255 per lane
                 acc[4 * k + 0] += (int)(lo[k] & 0xffff);
                 acc[4 * k + 2] += (int)(lo[k] >> 16);
                 acc[4 * k + 1] += (int)(hi[k] & 0xffff);
@@ -131,17 +138,21 @@ idd16_k(const uint4* __restrict__ tfb, int nchans, int nq16,
         }
     }
     const int bias = 128 * tscrunch * nchans;
-    uint32_t packed[4];
 #pragma unroll
-    for(int k = 0; k < 4; ++k) {
-        packed[k] = 0;
+    for(int u = 0; u < V; ++u) {
+        uint32_t packed[4];
 #pragma unroll
-        for(int b = 0; b < 4; ++b) {
-            const float v = fdiv((float)(acc[4 * k + b] - bias), scale_factor);
-            packed[k] |= ((uint32_t)(uint8_t)clamp_i8(v)) << (8 * b);
+        for(int k = 0; k < 4; ++k) {
+            packed[k] = 0;
+#pragma unroll
+            for(int b = 0; b < 4; ++b) {
+                const float v = fdiv((float)(acc[16 * u + 4 * k + b] - bias), scale_factor);
+                packed[k] |= ((uint32_t)(uint8_t)clamp_i8(v)) << (8 * b);
+            }
         }
+        tdb[((size_t)to * ndms + d) * nq16 + q + u] =
+            make_uint4(packed[0], packed[1], packed[2], packed[3]);
     }
-    tdb[((size_t)to * ndms + d) * nq16 + q] = make_uint4(packed[0], packed[1], packed[2], packed[3]);
 }
 
 }  // namespace
@@ -174,9 +185,9 @@ extern "C" int sw_incoherent_dedisperse(const int8_t* d_tfb, int nsamples,
     const long long chunk = 1ll << 30;  // blocks per launch (grid.x limit 2^31 - 1)
     for(long long b0 = 0; b0 < total; b0 += chunk) {
         const long long n = total - b0 < chunk ? total - b0 : chunk;
-        if(wide)
-            swb::idd16_k<<<(unsigned)n, 128, nchans * sizeof(long long), swb::as_cuda(stream)>>>(
-                reinterpret_cast<const uint4*>(d_tfb), nchans, nlanes, d_delays, max_delay,
+        if(wide)  // one 16-byte load per thread measured fastest (two: 129 -> 154 ms)
+            swb::idd16_k<1><<<(unsigned)n, 128, nchans * sizeof(long long), swb::as_cuda(stream)>>>(
+                reinterpret_cast<const uint4*>(d_tfb), nchans, nbeams / 16, d_delays, max_delay,
                 tscrunch, scale_factor, reinterpret_cast<uint4*>(d_tdb), ndms, nout, nqb,
                 group, b0);
         else
