@@ -328,7 +328,11 @@ def main_b200(args):
             "gpu_launches": launches * args.steps, "clocks": clocks}
     pipe.close()
     if not args.no_uhf:
-        line["uhf"] = uhf_case(torch, stages, synthetic, max(8, (args.steps + 3) // 4 * 4), 8)
+        free, _ = torch.cuda.mem_get_info()
+        if free >= 120e9:   # the UHF chain holds ~100 GB (aggregation buffers included)
+            line["uhf"] = uhf_case(torch, stages, synthetic, max(8, (args.steps + 3) // 4 * 4), 8)
+        else:
+            line["uhf"] = {"skipped": f"needs ~120 GB free device memory, {free / 1e9:.0f} GB free"}
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = {k: v for k, v in cpu_baseline().items() if k != "seconds"}
     if rank == 0:
