@@ -20,7 +20,8 @@
 // Roles (one CTA per SM, persistent over a ragged work queue):
 //   warp 0      TMA producer (weights double buffered, voltages 4 stages)
 //   warp 1      TMEM allocator + single-thread MMA issuer
-//   warps 2..9  epilogue (two warps per TMEM lane quarter)
+//   warps 2..   epilogue: 16 warps (four per TMEM lane quarter, 16 samples
+//               of each tile apiece), 8 for tscrunch 32
 // TMEM: 512 columns = 2 accumulator buffers x (D_re 128 | D_im 128).
 // Every wait is bounded by a kernel-wide deadline; on expiry the CTA records
 // DEV_ERR_CB_TIMEOUT in the device error word, stops issuing work and exits cleanly.
@@ -126,16 +127,30 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
                                           volatile int* abort_flag,
                                           unsigned long long deadline, int* err)
 {
-    uint32_t n = 0;
-    while(!mbar_try_wait(bar, parity)) {
-        if(*abort_flag) return false;
-        if((++n & 1023u) == 0 && globaltimer() > deadline) {
-            *abort_flag = 1;
-            if(err) atomicExch(err, DEV_ERR_CB_TIMEOUT);
-            return false;
+    if(mbar_try_wait(bar, parity)) return true;
+    // Slow path: suspend in the barrier (up to 20 us per poll, woken when the
+    // phase completes) instead of spinning, so that waiting warps do not take
+    // issue slots from the warps doing the work; the abort flag and the
+    // deadline are checked every 16 polls.
+    for(uint32_t n = 1;; ++n) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(ok)
+            : "r"(smem_u32(bar)), "r"(parity), "r"(20000u)
+            : "memory");
+        if(ok) return true;
+        if((n & 15u) == 0) {
+            if(*abort_flag) return false;
+            if(globaltimer() > deadline) {
+                *abort_flag = 1;
+                if(err) atomicExch(err, DEV_ERR_CB_TIMEOUT);
+                return false;
+            }
         }
     }
-    return true;
 }
 
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map,
@@ -193,14 +208,6 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar)
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-#define SW_TMEM_LD16(taddr, r)                                                             \
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 "                                 \
-                 "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"        \
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), \
-                   "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]),            \
-                   "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])         \
-                 : "r"(taddr))
-
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 #define SW_TMEM_LD8(taddr, r)                                                              \
@@ -208,22 +215,6 @@ __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.
                  : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),  \
                    "=r"(r[6]), "=r"(r[7])                                                   \
                  : "r"(taddr))
-
-#define SW_TMEM_ST8(taddr, r)                                                              \
-    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};"   \
-                 ::"r"(taddr), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]),         \
-                 "r"(r[5]), "r"(r[6]), "r"(r[7])                                              \
-                 : "memory")
-
-#define SW_TMEM_ST16(taddr, r)                                                              \
-    asm volatile("tcgen05.st.sync.aligned.32x32b.x16.b32 "                                  \
-                 "[%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(taddr), \
-                 "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]),  \
-                 "r"(r[7]), "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]),          \
-                 "r"(r[13]), "r"(r[14]), "r"(r[15])                                            \
-                 : "memory")
-
-__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
 // ------------------------------------------------- exact packed arithmetic
 // Pairs of IEEE single operations (.rn, never contracted into an FMA), so
@@ -349,7 +340,10 @@ __device__ __forceinline__ Item decode(const Params& P, int item)
     return it;
 }
 
-template <int TS, int STOKES>
+// DBG instances also write the exact int32 beam voltages to P.debug; the
+// production instances carry no debug path (it costs ~20 registers and a
+// branch per load group).
+template <int TS, int STOKES, bool DBG>
 __global__ void __launch_bounds__(cb_threads<TS>(), 1)
 cb_kernel(const __grid_constant__ Params P)
 {
@@ -462,8 +456,7 @@ cb_kernel(const __grid_constant__ Params P)
     } else {
         // ------------------------------------------------------ epilogue
         constexpr int kSlice  = TS > 16 ? 32 : 16;   // samples per warp per tile
-        // 8 TMEM columns per load group: x16 groups need more registers than
-        // the 18-warp launch leaves (they spill at the 96 the launch allows)
+        // 8 TMEM columns per load group, two groups in registers at a time
         constexpr int kG      = 8;
         constexpr int kGroups = kSlice / kG;         // column groups per warp
         const int q = warp & 3;          // TMEM lane quarter of this warp
@@ -489,9 +482,17 @@ cb_kernel(const __grid_constant__ Params P)
             const int tile1 = min(ntiles_gulp, tile0 + P.tpi);
             bool ok = true;
             constexpr int NC = STOKES == 4 ? 4 : 1;  // output components
+            constexpr int kEmits = kSlice / TS;      // outputs per warp per tile
+            // Output and IB-power elements of this warp's first output in
+            // tile0; both advance by kTileT / TS output samples per tile.
+            const int to0 = (tile0 * kTileT + h * kSlice) / TS;
+            int8_t* outp = pr.out + (((size_t)to0 * F + it.f) * P.nbeams + b) * NC;
+            const float* ibq =
+                P.ib_subtract ? pr.ib_raw + (((size_t)bs * nout + to0) * F + it.f) * NC : nullptr;
+            const size_t out_emit = (size_t)F * P.nbeams * NC;  // next output sample
+            const size_t ib_emit  = (size_t)F * NC;
             // IB powers of this warp's outputs in the tile, fetched before the
             // accumulator wait so that their latency hides behind it
-            constexpr int kEmits = kSlice / TS;
             constexpr bool kPrefetch = kEmits * NC <= 4;
             float ibp[kPrefetch ? kEmits * NC : 1];
             for(int tile = tile0; tile < tile1; ++tile) {
@@ -499,12 +500,10 @@ cb_kernel(const __grid_constant__ Params P)
                     if(P.ib_subtract) {
 #pragma unroll
                         for(int e = 0; e < kEmits; ++e) {
-                            const int to = (tile * kTileT + h * kSlice + (e + 1) * TS - 1) / TS;
-                            const size_t ii = ((size_t)bs * nout + to) * F + it.f;
                             if constexpr(NC == 1) {
-                                ibp[e] = pr.ib_raw[ii];
+                                ibp[e] = ibq[e * ib_emit];
                             } else {
-                                const float4 v = reinterpret_cast<const float4*>(pr.ib_raw)[ii];
+                                const float4 v = reinterpret_cast<const float4*>(ibq)[e * F];
                                 ibp[4 * e] = v.x; ibp[4 * e + 1] = v.y;
                                 ibp[4 * e + 2] = v.z; ibp[4 * e + 3] = v.w;
                             }
@@ -516,24 +515,31 @@ cb_kernel(const __grid_constant__ Params P)
                 float power[NC];  // carried across groups while tscrunch > 8
 #pragma unroll
                 for(int c = 0; c < NC; ++c) power[c] = 0.0f;
+                // Column groups are loaded one ahead of the arithmetic:
+                // group g + 1's TMEM loads are in flight while group g is
+                // reduced (tcgen05.wait::ld then waits for them).
+                const uint32_t ta0 = lane_base + ab * 256 + h * kSlice;
+                uint32_t rr[2][4][kG];  // [buffer][Re p0, Re p1, Im p0, Im p1][column]
+                SW_TMEM_LD8(ta0, rr[0][0]);
+                SW_TMEM_LD8(ta0 + 64, rr[0][1]);
+                SW_TMEM_LD8(ta0 + 128, rr[0][2]);
+                SW_TMEM_LD8(ta0 + 192, rr[0][3]);
+                tmem_wait_ld();
 #pragma unroll
                 for(int g = 0; g < kGroups; ++g) {
-                    const uint32_t ta = lane_base + ab * 256 + h * kSlice + g * kG;
-                    uint32_t r0[kG], r1[kG], i0[kG], i1[kG];
-                    if constexpr(kG == 16) {
-                        SW_TMEM_LD16(ta, r0);
-                        SW_TMEM_LD16(ta + 64, r1);
-                        SW_TMEM_LD16(ta + 128, i0);
-                        SW_TMEM_LD16(ta + 192, i1);
-                    } else {
-                        SW_TMEM_LD8(ta, r0);
-                        SW_TMEM_LD8(ta + 64, r1);
-                        SW_TMEM_LD8(ta + 128, i0);
-                        SW_TMEM_LD8(ta + 192, i1);
+                    if(g + 1 < kGroups) {
+                        const uint32_t ta = ta0 + (g + 1) * kG;
+                        SW_TMEM_LD8(ta, rr[(g + 1) & 1][0]);
+                        SW_TMEM_LD8(ta + 64, rr[(g + 1) & 1][1]);
+                        SW_TMEM_LD8(ta + 128, rr[(g + 1) & 1][2]);
+                        SW_TMEM_LD8(ta + 192, rr[(g + 1) & 1][3]);
                     }
-                    tmem_wait_ld();
+                    const uint32_t* r0 = rr[g & 1][0];
+                    const uint32_t* r1 = rr[g & 1][1];
+                    const uint32_t* i0 = rr[g & 1][2];
+                    const uint32_t* i1 = rr[g & 1][3];
                     const int tbase = tile * kTileT + h * kSlice + g * kG;
-                    if(P.debug != nullptr && valid) {
+                    if(DBG && valid) {
                         int2* dbg = reinterpret_cast<int2*>(P.debug);
                         for(int t = 0; t < kG; ++t) {
                             const size_t base_t = (size_t)it.f * P.nsamples + tbase + t;
@@ -553,28 +559,25 @@ cb_kernel(const __grid_constant__ Params P)
                         const int u = g * kG + t;  // sample within this warp's slice
                         const bool emit = ((u + 1) % TS) == 0;
                         if(emit) {
-                            const int to = (tbase + t) / TS;
-                            const size_t ii = ((size_t)bs * nout + to) * F + it.f;
-                            const size_t oi = ((size_t)to * F + it.f) * P.nbeams + b;
                             const int e = u / TS;  // emit index within the slice
                             if constexpr(NC == 1) {
                                 float v;
                                 if(P.ib_subtract) {
-                                    const float ib = kPrefetch ? ibp[kPrefetch ? e : 0] : pr.ib_raw[ii];
+                                    const float ib = kPrefetch ? ibp[kPrefetch ? e : 0] : ibq[e * ib_emit];
                                     v = rintf(fdiv(fsub(power[0], fmul(ib, 16129.0f)), scale));
                                 } else if(STOKES == 0) {
                                     v = rintf(fdiv(fsub(power[0], offs), scale));
                                 } else {
                                     v = rintf(fdiv(power[0], scale));
                                 }
-                                if(valid) pr.out[oi] = clamp_i8(v);
+                                if(valid) outp[e * out_emit] = clamp_i8(v);
                             } else {
                                 // char4 {I, Q, U, V}; the IB power is float4
                                 float v[4];
                                 if(P.ib_subtract) {
                                     const float4 ib = kPrefetch
                                         ? make_float4(ibp[0], ibp[1], ibp[2], ibp[3])
-                                        : reinterpret_cast<const float4*>(pr.ib_raw)[ii];
+                                        : reinterpret_cast<const float4*>(ibq)[e * F];
                                     v[0] = rintf(fdiv(fsub(power[0], fmul(ib.x, 16129.0f)), scale));
                                     v[1] = rintf(fdiv(fsub(power[1], fmul(ib.y, 16129.0f)), scale));
                                     v[2] = rintf(fdiv(fsub(power[2], fmul(ib.z, 16129.0f)), scale));
@@ -586,7 +589,7 @@ cb_kernel(const __grid_constant__ Params P)
                                     v[3] = rintf(fdiv(power[3], scale));
                                 }
                                 if(valid)
-                                    reinterpret_cast<char4*>(pr.out)[oi] =
+                                    reinterpret_cast<char4*>(outp)[e * F * P.nbeams] =
                                         make_char4(clamp_i8(v[0]), clamp_i8(v[1]),
                                                    clamp_i8(v[2]), clamp_i8(v[3]));
                             }
@@ -594,11 +597,14 @@ cb_kernel(const __grid_constant__ Params P)
                             for(int c = 0; c < NC; ++c) power[c] = 0.0f;
                         }
                     }
+                    if(g + 1 < kGroups) tmem_wait_ld();
                 }
                 fence_before();
                 __syncwarp();
                 if(lane == 0) mbar_arrive(&acc_empty[ab]);
                 if(++ab == 2) { ab = 0; aph ^= 1; }
+                outp += (kTileT / TS) * out_emit;
+                if(P.ib_subtract) ibq += (kTileT / TS) * ib_emit;
             }
             if(!ok) break;
         }
@@ -790,14 +796,21 @@ int launch(const sw_cb_shape* s, const sw_cb_problem* probs, int nprob,
     return dispatch_ts(s->tscrunch, s->stokes, grid, smem, stream);
 }
 
+template <int TS, int STOKES, bool DBG>
+int launch_instance(int grid, size_t smem, cudaStream_t stream)
+{
+    SW_CUDA_CHECK(cudaFuncSetAttribute(cb_kernel<TS, STOKES, DBG>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    cb_kernel<TS, STOKES, DBG><<<grid, cb_threads<TS>(), smem, stream>>>(launch_params());
+    SW_LAUNCH_CHECK();
+    return SW_OK;
+}
+
 template <int TS, int STOKES>
 int launch_variant(int grid, size_t smem, cudaStream_t stream)
 {
-    SW_CUDA_CHECK(cudaFuncSetAttribute(cb_kernel<TS, STOKES>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    cb_kernel<TS, STOKES><<<grid, cb_threads<TS>(), smem, stream>>>(launch_params());
-    SW_LAUNCH_CHECK();
-    return SW_OK;
+    return launch_params().debug != nullptr ? launch_instance<TS, STOKES, true>(grid, smem, stream)
+                                            : launch_instance<TS, STOKES, false>(grid, smem, stream);
 }
 
 template <int TS>
