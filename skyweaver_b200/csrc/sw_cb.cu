@@ -97,10 +97,12 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
 }
 
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
+// Barrier and copy helpers take shared-window addresses (uint32_t), so that
+// the single-thread producer and MMA roles step through their stages with
+// plain adds.
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes)
 {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-                 "r"(bytes)
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
                  : "memory");
 }
 
@@ -109,7 +111,7 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar)
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity)
 {
     uint32_t ok;
     asm volatile(
@@ -117,14 +119,14 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
         "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}\n"
         : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
+        : "r"(bar), "r"(parity)
         : "memory");
     return ok != 0;
 }
 
 // Bounded wait: false if the kernel-wide deadline passed or another role
 // already aborted.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity,
                                           volatile int* abort_flag,
                                           unsigned long long deadline, int* err)
 {
@@ -140,7 +142,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
             "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
             "selp.u32 %0, 1, 0, p;\n\t}\n"
             : "=r"(ok)
-            : "r"(smem_u32(bar)), "r"(parity), "r"(20000u)
+            : "r"(bar), "r"(parity), "r"(20000u)
             : "memory");
         if(ok) return true;
         if((n & 15u) == 0) {
@@ -154,23 +156,23 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
     }
 }
 
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map,
-                                            uint64_t* bar, int x, int y)
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map,
+                                            uint32_t bar, int x, int y)
 {
     asm volatile(
         "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
-        "[%0], [%1, {%3, %4}], [%2];" ::"r"(smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
+        "[%0], [%1, {%3, %4}], [%2];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(x), "r"(y)
         : "memory");
 }
 
-__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map,
-                                            uint64_t* bar, int x, int y, int z)
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map,
+                                            uint32_t bar, int x, int y, int z)
 {
     asm volatile(
         "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
-        "[%0], [%1, {%3, %4, %5}], [%2];" ::"r"(smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z)
+        "[%0], [%1, {%3, %4, %5}], [%2];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(x), "r"(y), "r"(z)
         : "memory");
 }
 
@@ -220,11 +222,10 @@ __device__ __forceinline__ void mma_tile(uint32_t d_re, uint32_t a_re, uint32_t 
     }
 }
 
-__device__ __forceinline__ void mma_commit(uint64_t* bar)
+__device__ __forceinline__ void mma_commit(uint32_t bar)
 {
     asm volatile(
-        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-            smem_u32(bar))
+        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
         : "memory");
 }
 
@@ -388,6 +389,10 @@ cb_kernel(const __grid_constant__ Params P)
     uint32_t* s_tmem    = reinterpret_cast<uint32_t*>(acc_empty + 2);
     volatile int* s_abort = reinterpret_cast<volatile int*>(s_tmem + 1);
 
+    // shared-window addresses: barrier k of an array is at base + 8 k
+    const uint32_t v_full_s = smem_u32(v_full), v_empty_s = smem_u32(v_empty);
+    const uint32_t w_full_s = smem_u32(w_full), w_empty_s = smem_u32(w_empty);
+    const uint32_t acc_full_s = smem_u32(acc_full), acc_empty_s = smem_u32(acc_empty);
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const unsigned long long deadline = globaltimer() + P.timeout_ns;
@@ -414,24 +419,28 @@ cb_kernel(const __grid_constant__ Params P)
     if(warp == 0) {
         if(lane == 0) {
             // ---------------------------------------------------- producer
+            const uint32_t wbuf_s = smem_u32(wbuf), vbuf_s = smem_u32(vbuf);
             int vs = 0, ws = 0;
             uint32_t vph = 0, wph = 0;
             for(int item = blockIdx.x; item < P.nitems && !*s_abort; item += gridDim.x) {
                 const Item it = decode(P, item);
                 const Problem& pr = P.prob[it.p];
-                if(!mbar_wait(&w_empty[ws], wph ^ 1, s_abort, deadline, P.err)) break;
-                mbar_expect_tx(&w_full[ws], 2 * wtile);
-                uint8_t* wdst = wbuf + ws * 2 * wtile;
-                tma_load_2d(wdst, &P.wmap, &w_full[ws], 0, (it.f * 2 + 0) * P.nbeams + it.b0);
-                tma_load_2d(wdst + wtile, &P.wmap, &w_full[ws], 0, (it.f * 2 + 1) * P.nbeams + it.b0);
+                if(!mbar_wait(w_empty_s + 8 * ws, wph ^ 1, s_abort, deadline, P.err)) break;
+                const uint32_t wbar = w_full_s + 8 * ws;
+                mbar_expect_tx(wbar, 2 * wtile);
+                const uint32_t wdst = wbuf_s + ws * 2 * wtile;
+                tma_load_2d(wdst, &P.wmap, wbar, 0, (it.f * 2 + 0) * P.nbeams + it.b0);
+                tma_load_2d(wdst + wtile, &P.wmap, wbar, 0, (it.f * 2 + 1) * P.nbeams + it.b0);
                 if(++ws == kWStages) { ws = 0; wph ^= 1; }
                 const int tile0 = it.tc * P.tpi;
                 const int tile1 = min(ntiles_gulp, tile0 + P.tpi);
-                for(int tile = tile0; tile < tile1; ++tile) {
-                    if(!mbar_wait(&v_empty[vs], vph ^ 1, s_abort, deadline, P.err)) break;
-                    mbar_expect_tx(&v_full[vs], vtile);
-                    tma_load_3d(vbuf + vs * vtile, &P.vmap[pr.dm], &v_full[vs],
-                                (int)(P.sample_offset + (size_t)tile * kTileT), 0, it.f * 2);
+                const CUtensorMap* vmap = &P.vmap[pr.dm];
+                int x = (int)(P.sample_offset + (size_t)tile0 * kTileT);
+                for(int tile = tile0; tile < tile1; ++tile, x += kTileT) {
+                    if(!mbar_wait(v_empty_s + 8 * vs, vph ^ 1, s_abort, deadline, P.err)) break;
+                    const uint32_t vbar = v_full_s + 8 * vs;
+                    mbar_expect_tx(vbar, vtile);
+                    tma_load_3d(vbuf_s + vs * vtile, vmap, vbar, x, 0, it.f * 2);
                     if(++vs == kVStages) { vs = 0; vph ^= 1; }
                 }
             }
@@ -452,29 +461,29 @@ cb_kernel(const __grid_constant__ Params P)
             const uint32_t b_lo0 = desc_lo(smem_u32(vbuf), P.v_lbo16);
             for(int item = blockIdx.x; item < P.nitems && !*s_abort; item += gridDim.x) {
                 const Item it = decode(P, item);
-                if(!mbar_wait(&w_full[ws], wph, s_abort, deadline, P.err)) break;
+                if(!mbar_wait(w_full_s + 8 * ws, wph, s_abort, deadline, P.err)) break;
                 const uint32_t a_re = a_lo0 + ((ws * 2 * wtile) >> 4);
                 const uint32_t a_im = a_re + (wtile >> 4);
                 const int tile0 = it.tc * P.tpi;
                 const int tile1 = min(ntiles_gulp, tile0 + P.tpi);
                 bool ok = true;
                 for(int tile = tile0; tile < tile1; ++tile) {
-                    if(!mbar_wait(&v_full[vs], vph, s_abort, deadline, P.err)) { ok = false; break; }
+                    if(!mbar_wait(v_full_s + 8 * vs, vph, s_abort, deadline, P.err)) { ok = false; break; }
                     // phase 0 of acc_empty is completed by the epilogue
                     // warps' initial arrival (both buffers start free)
-                    if(!mbar_wait(&acc_empty[ab], aph, s_abort, deadline, P.err)) { ok = false; break; }
+                    if(!mbar_wait(acc_empty_s + 8 * ab, aph, s_abort, deadline, P.err)) { ok = false; break; }
                     fence_after();
                     const uint32_t b_lo = b_lo0 + ((vs * vtile) >> 4);
                     const uint32_t d_re = tmem + ab * 256;  // D_im at d_re + 128
                     if(ksteps == 4) mma_tile<4>(d_re, a_re, a_im, a_hi, b_lo, b_hi, P.idesc);
                     else if(ksteps == 2) mma_tile<2>(d_re, a_re, a_im, a_hi, b_lo, b_hi, P.idesc);
                     else mma_tile<1>(d_re, a_re, a_im, a_hi, b_lo, b_hi, P.idesc);
-                    mma_commit(&v_empty[vs]);
-                    mma_commit(&acc_full[ab]);
+                    mma_commit(v_empty_s + 8 * vs);
+                    mma_commit(acc_full_s + 8 * ab);
                     if(++vs == kVStages) { vs = 0; vph ^= 1; }
                     if(++ab == 2) { ab = 0; aph ^= 1; }
                 }
-                mma_commit(&w_empty[ws]);
+                mma_commit(w_empty_s + 8 * ws);
                 if(++ws == kWStages) { ws = 0; wph ^= 1; }
                 if(!ok) break;
             }
@@ -540,7 +549,7 @@ cb_kernel(const __grid_constant__ Params P)
                             }
                         }
                     }
-                    if(!mbar_wait(&acc_full[ab], aph, s_abort, deadline, P.err)) { ok = false; break; }
+                    if(!mbar_wait(acc_full_s + 8 * ab, aph, s_abort, deadline, P.err)) { ok = false; break; }
                     fence_after();
                     float power[NC];  // carried across groups while tscrunch > 8
 #pragma unroll
