@@ -234,6 +234,14 @@ __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::aft
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
+#define SW_TMEM_LD16(taddr, r)                                                             \
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 "                                 \
+                 "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"        \
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), \
+                   "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]),            \
+                   "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])         \
+                 : "r"(taddr))
+
 #define SW_TMEM_LD8(taddr, r)                                                              \
     asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"    \
                  : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),  \
@@ -491,8 +499,10 @@ cb_kernel(const __grid_constant__ Params P)
     } else {
         // ------------------------------------------------------ epilogue
         constexpr int kSlice  = 32;                  // samples per warp per tile
-        // 8 TMEM columns per load group, two groups in registers at a time
-        constexpr int kG      = 8;
+        // TMEM columns per load group: 16 (measured 1.5 % faster than 8),
+        // except for full Stokes at tscrunch <= 4, whose many outputs per
+        // group leave too few registers for it
+        constexpr int kG      = (STOKES == 4 && TS <= 4) ? 8 : 16;
         constexpr int kGroups = kSlice / kG;         // column groups per warp
         const int q   = warp & 3;               // TMEM lane quarter of this warp
         const int h   = ((warp - 2) >> 2) & 1;  // which half of the tile's 64 samples
@@ -562,10 +572,17 @@ cb_kernel(const __grid_constant__ Params P)
                     for(int g = 0; g < kGroups; ++g) {
                         uint32_t r0[kG], r1[kG], i0[kG], i1[kG];
                         const uint32_t ta = ta0 + g * kG;
-                        SW_TMEM_LD8(ta, r0);
-                        SW_TMEM_LD8(ta + 64, r1);
-                        SW_TMEM_LD8(ta + 128, i0);
-                        SW_TMEM_LD8(ta + 192, i1);
+                        if constexpr(kG == 16) {
+                            SW_TMEM_LD16(ta, r0);
+                            SW_TMEM_LD16(ta + 64, r1);
+                            SW_TMEM_LD16(ta + 128, i0);
+                            SW_TMEM_LD16(ta + 192, i1);
+                        } else {
+                            SW_TMEM_LD8(ta, r0);
+                            SW_TMEM_LD8(ta + 64, r1);
+                            SW_TMEM_LD8(ta + 128, i0);
+                            SW_TMEM_LD8(ta + 192, i1);
+                        }
                         tmem_wait_ld();
                         const int tbase = tile * kTileT + h * kSlice + g * kG;
                         if(DBG && valid) {
