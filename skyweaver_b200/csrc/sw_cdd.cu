@@ -203,6 +203,13 @@ __device__ __forceinline__ void dft(c32* x)
 // one padding slot per 16 complex values keeps the strided radix-16 passes
 // free of shared-memory bank conflicts
 __host__ __device__ constexpr int pad(int i) { return i + (i >> 4); }
+// pad(b + q * s) for a stride s that is a multiple of 16: the padding of
+// b + q s is pad(b) + q (s + s / 16), i.e. one base plus constant offsets
+// (the compiler folds them into the shared-memory instructions).
+__device__ __forceinline__ int pad_at(int b, int pb, int q, int s)
+{
+    return (s & 15) == 0 ? pb + q * (s + (s >> 4)) : pad(b + q * s);
+}
 
 struct Args {
     const uint8_t* in;
@@ -251,9 +258,10 @@ __device__ __forceinline__ void inv_pass(c32* buf, const c32* tw_s, int G, int s
         const int beta = threadIdx.x + u * NT;
         const int g = beta / s, j = beta - g * s;
         const int base = g * G + j;
+        const int pb = pad(base);
         c32 z[R];
 #pragma unroll
-        for(int q = 0; q < R; ++q) z[q] = buf[pad(base + q * s)];
+        for(int q = 0; q < R; ++q) z[q] = buf[pad_at(base, pb, q, s)];
         if(s > 1) {
 {
                 c32 w[R];
@@ -264,7 +272,7 @@ __device__ __forceinline__ void inv_pass(c32* buf, const c32* tw_s, int G, int s
         }
         dft<R, true>(z);
 #pragma unroll
-        for(int r = 0; r < R; ++r) buf[pad(base + r * s)] = z[r];
+        for(int r = 0; r < R; ++r) buf[pad_at(base, pb, r, s)] = z[r];
     }
 }
 
@@ -280,9 +288,10 @@ __device__ __forceinline__ void fwd_pass(c32* buf, const c32* tw_s, int G, int s
         const int beta = threadIdx.x + u * NT;
         const int g = beta / s, j = beta - g * s;
         const int base = g * G + j;
+        const int pb = pad(base);
         c32 x[R];
 #pragma unroll
-        for(int r = 0; r < R; ++r) x[r] = buf[pad(base + r * s)];
+        for(int r = 0; r < R; ++r) x[r] = buf[pad_at(base, pb, r, s)];
         dft<R, false>(x);
         if(s > 1) {
 {
@@ -293,7 +302,7 @@ __device__ __forceinline__ void fwd_pass(c32* buf, const c32* tw_s, int G, int s
             }
         }
 #pragma unroll
-        for(int q = 0; q < R; ++q) buf[pad(base + q * s)] = x[q];
+        for(int q = 0; q < R; ++q) buf[pad_at(base, pb, q, s)] = x[q];
     }
 }
 
@@ -391,7 +400,7 @@ cdd_kernel(const __grid_constant__ Args A)
                     for(int q = 1; q < R0; ++q) x[q] = cmul(x[q], w[q]);
                 }
 #pragma unroll
-                for(int q = 0; q < R0; ++q) buf[pad(j + q * s0)] = x[q];
+                for(int q = 0; q < R0; ++q) buf[pad_at(j, pad(j), q, s0)] = x[q];
             }
         }
         __syncthreads();
@@ -448,7 +457,7 @@ cdd_kernel(const __grid_constant__ Args A)
                 const int j = threadIdx.x + u * NT;
                 c32 z[R0];
 #pragma unroll
-                for(int q = 0; q < R0; ++q) z[q] = buf[pad(j + q * s0)];
+                for(int q = 0; q < R0; ++q) z[q] = buf[pad_at(j, pad(j), q, s0)];
 {
                     c32 w[R0];
                     load_tw<R0>(tw_s, P.tw_off[0], s0, j, w);
@@ -607,7 +616,7 @@ cdd_split_kernel(const __grid_constant__ SplitArgs A)
                 const int j = threadIdx.x + v * NT;
                 c32 z[R0];
 #pragma unroll
-                for(int q = 0; q < R0; ++q) z[q] = buf[pad(j + q * s0)];
+                for(int q = 0; q < R0; ++q) z[q] = buf[pad_at(j, pad(j), q, s0)];
                 {
                     c32 w[R0];
                     load_tw<R0>(tw_s, P.tw_off[0], s0, j, w);
