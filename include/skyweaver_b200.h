@@ -66,6 +66,14 @@ const char* sw_last_error(void);
 int sw_read_device_error(int* h_code);
 int sw_reset_device_error(void);
 
+/* Bounded-wait self-test of the coherent beamformer (no reference
+ * counterpart: the reference has no device-side waits).  Launches a minimal
+ * beamformer whose copy producer issues nothing, so its MMA role's first wait
+ * can only end at the given deadline (microseconds, at most 10 s).  Returns
+ * SW_ERR_TIMEOUT when the kernel recorded the timeout in the device error
+ * word and returned (the word is cleared again), SW_ERR_STATE if it did not. */
+int sw_cb_timeout_selftest(int timeout_us, sw_stream_t stream);
+
 /* ------------------------------------------------------------------ */
 /* Transposer                                                           */
 /* ------------------------------------------------------------------ */

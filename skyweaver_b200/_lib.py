@@ -16,6 +16,7 @@ c_void_p = ctypes.c_void_p
 c_float_p = ctypes.POINTER(ctypes.c_float)
 
 SW_OK = 0
+SW_ERR_TIMEOUT = 4  # a bounded device-side wait gave up
 IDD_HANDLER = ctypes.CFUNCTYPE(None, c_void_p, c_int, c_void_p, c_int, c_int, c_int, c_void_p)
 STOKES = {"I": 0, "Q": 1, "U": 2, "V": 3, "IQUV": 4}
 
@@ -63,6 +64,7 @@ _SIGS = {
     "sw_last_error": (ctypes.c_char_p, []),
     "sw_read_device_error": (c_int, [ctypes.POINTER(c_int)]),
     "sw_reset_device_error": (c_int, []),
+    "sw_cb_timeout_selftest": (c_int, [c_int, c_void_p]),
     "sw_transpose_ftpa": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_void_p]),
     "sw_transpose_fpact": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int,
                                    c_size_t, c_size_t, c_void_p]),

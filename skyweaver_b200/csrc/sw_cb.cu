@@ -77,6 +77,7 @@ struct Params {
     uint32_t idesc;
     uint32_t w_layout, w_sbo16, v_lbo16;
     unsigned long long timeout_ns;
+    int test_stall;  // self-test: the producer issues nothing, so waits run out
 };
 
 // ------------------------------------------------------------ PTX helpers
@@ -394,7 +395,8 @@ cb_kernel(const __grid_constant__ Params P)
     uint64_t* w_empty   = w_full + kWStages;
     uint64_t* acc_full  = w_empty + kWStages;
     uint64_t* acc_empty = acc_full + 2;
-    uint32_t* s_tmem    = reinterpret_cast<uint32_t*>(acc_empty + 2);
+    uint64_t* drain     = acc_empty + 2;  // MMA completion on abort
+    uint32_t* s_tmem    = reinterpret_cast<uint32_t*>(drain + 1);
     volatile int* s_abort = reinterpret_cast<volatile int*>(s_tmem + 1);
 
     // shared-window addresses: barrier k of an array is at base + 8 k
@@ -409,6 +411,7 @@ cb_kernel(const __grid_constant__ Params P)
         for(int i = 0; i < kVStages; ++i) { mbar_init(&v_full[i], 1); mbar_init(&v_empty[i], 1); }
         for(int i = 0; i < kWStages; ++i) { mbar_init(&w_full[i], 1); mbar_init(&w_empty[i], 1); }
         for(int i = 0; i < 2; ++i) { mbar_init(&acc_full[i], 1); mbar_init(&acc_empty[i], kEpiWarps / 2); }
+        mbar_init(drain, 1);
         *s_abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -425,17 +428,21 @@ cb_kernel(const __grid_constant__ Params P)
     const int ntiles_gulp = P.nsamples / kTileT;
 
     if(warp == 0) {
-        if(lane == 0) {
+        if(lane == 0 && !P.test_stall) {
             // ---------------------------------------------------- producer
             const uint32_t wbuf_s = smem_u32(wbuf), vbuf_s = smem_u32(vbuf);
             int vs = 0, ws = 0;
             uint32_t vph = 0, wph = 0;
+            // stages armed so far and the phase parity of each one's last arm
+            uint32_t v_armed = 0, v_par = 0, w_armed = 0, w_par = 0;
             for(int item = blockIdx.x; item < P.nitems && !*s_abort; item += gridDim.x) {
                 const Item it = decode(P, item);
                 const Problem& pr = P.prob[it.p];
                 if(!mbar_wait(w_empty_s + 8 * ws, wph ^ 1, s_abort, deadline, P.err)) break;
                 const uint32_t wbar = w_full_s + 8 * ws;
                 mbar_expect_tx(wbar, 2 * wtile);
+                w_armed |= 1u << ws;
+                w_par = (w_par & ~(1u << ws)) | (wph << ws);
                 const uint32_t wdst = wbuf_s + ws * 2 * wtile;
                 tma_load_2d(wdst, &P.wmap, wbar, 0, (it.f * 2 + 0) * P.nbeams + it.b0);
                 tma_load_2d(wdst + wtile, &P.wmap, wbar, 0, (it.f * 2 + 1) * P.nbeams + it.b0);
@@ -448,9 +455,23 @@ cb_kernel(const __grid_constant__ Params P)
                     if(!mbar_wait(v_empty_s + 8 * vs, vph ^ 1, s_abort, deadline, P.err)) break;
                     const uint32_t vbar = v_full_s + 8 * vs;
                     mbar_expect_tx(vbar, vtile);
+                    v_armed |= 1u << vs;
+                    v_par = (v_par & ~(1u << vs)) | (vph << vs);
                     tma_load_3d(vbuf_s + vs * vtile, vmap, vbar, x, 0, it.f * 2);
                     if(++vs == kVStages) { vs = 0; vph ^= 1; }
                 }
+            }
+            // After an abort, let every copy still in flight land before the
+            // CTA exits (each stage's last armed phase completes when its
+            // bytes arrive; bounded like every other wait).
+            if(*s_abort) {
+                const unsigned long long until = globaltimer() + 100ull * 1000 * 1000;
+                for(int i = 0; i < kVStages; ++i)
+                    if(v_armed >> i & 1)
+                        while(!mbar_try_wait(v_full_s + 8 * i, v_par >> i & 1) && globaltimer() < until) {}
+                for(int i = 0; i < kWStages; ++i)
+                    if(w_armed >> i & 1)
+                        while(!mbar_try_wait(w_full_s + 8 * i, w_par >> i & 1) && globaltimer() < until) {}
             }
         }
     } else if(warp == 1) {
@@ -494,6 +515,15 @@ cb_kernel(const __grid_constant__ Params P)
                 mma_commit(w_empty_s + 8 * ws);
                 if(++ws == kWStages) { ws = 0; wph ^= 1; }
                 if(!ok) break;
+            }
+            // After an abort, wait (bounded) for the MMAs already issued, so
+            // that none is still reading shared memory or writing TMEM when
+            // the CTA frees them.
+            if(*s_abort) {
+                const uint32_t drain_s = smem_u32(drain);
+                mma_commit(drain_s);
+                const unsigned long long until = globaltimer() + 100ull * 1000 * 1000;
+                while(!mbar_try_wait(drain_s, 0) && globaltimer() < until) {}
             }
         }
     } else {
@@ -736,7 +766,7 @@ int dispatch_ts(int ts, int stokes, int grid, size_t smem, cudaStream_t stream);
 size_t smem_bytes(int kbytes)
 {
     return 1024 + (size_t)kWStages * 2 * kM * kbytes + (size_t)kVStages * 2 * kbytes * kTileT +
-           (2 * kVStages + 2 * kWStages + 4) * 8 + 16;
+           (2 * kVStages + 2 * kWStages + 5) * 8 + 16;
 }
 
 int num_sms()
@@ -753,7 +783,8 @@ int num_sms()
 
 int launch(const sw_cb_shape* s, const sw_cb_problem* probs, int nprob,
            const void* w, const float* scale, const float* offset,
-           const int* mapping, int32_t* debug, cudaStream_t stream)
+           const int* mapping, int32_t* debug, cudaStream_t stream,
+           unsigned long long timeout_ns = 5ull * 1000 * 1000 * 1000, int test_stall = 0)
 {
     SW_REQUIRE(s && probs && nprob > 0 && w && scale && offset && mapping,
                "CoherentBeamformer: null argument");
@@ -835,7 +866,8 @@ int launch(const sw_cb_shape* s, const sw_cb_problem* probs, int nprob,
     P.w_layout = P.kbytes == 128 ? 2u : P.kbytes == 64 ? 4u : 6u;  // SW128/SW64/SW32
     P.w_sbo16  = (uint32_t)(8 * P.kbytes / 16);                       // 8-row group stride
     P.v_lbo16  = (uint32_t)(2 * s->nantennas * kTileT / 16);          // pol plane stride
-    P.timeout_ns = 5ull * 1000 * 1000 * 1000;                         // 5 s
+    P.timeout_ns = timeout_ns;                                        // 5 s by default
+    P.test_stall = test_stall;
 
     const size_t smem = smem_bytes(P.kbytes);
     const int grid = P.nitems < num_sms() ? P.nitems : num_sms();
@@ -905,6 +937,69 @@ int sw_coherent_beamform_grouped(const sw_cb_shape* shape,
 {
     return swb::cb::launch(shape, h_problems, nproblems, d_weights_gemm, d_scale, d_offset,
                            d_mapping, nullptr, swb::as_cuda(stream));
+}
+
+// Bounded-wait self-test: a minimal grouped launch (16 antennas, 1 channel,
+// 128 beams, 64 samples) whose producer issues no copies, so the MMA role's
+// first weights wait can only end at its deadline.  The kernel must record
+// its timeout in the device error word and return; the context stays usable.
+int sw_cb_timeout_selftest(int timeout_us, sw_stream_t stream)
+{
+    SW_REQUIRE(timeout_us > 0 && timeout_us <= 10 * 1000 * 1000,
+               "sw_cb_timeout_selftest: timeout must be in (0, 10 s]");
+    const cudaStream_t st = swb::as_cuda(stream);
+    sw_cb_shape shape{};
+    shape.nantennas = 16;
+    shape.nbeams = 128;
+    shape.nchans = 1;
+    shape.nsamples = 64;
+    shape.tscrunch = 16;
+    shape.stokes = 0;
+    shape.ib_subtract = 1;
+    shape.row_stride = 64;
+    shape.sample_offset = 0;
+    const size_t v_bytes = (size_t)shape.row_stride * 2 * shape.nantennas * 2 * shape.nchans;
+    const size_t w_bytes = (size_t)shape.nchans * 2 * shape.nbeams * 2 * shape.nantennas;
+    void *v = nullptr, *w = nullptr, *f = nullptr, *o = nullptr, *m = nullptr;
+    int rc = SW_OK;
+    auto fail = [](int code, const char* msg) {
+        swb::set_error("sw_cb_timeout_selftest: %s", msg);
+        return code;
+    };
+    if(cudaMalloc(&v, v_bytes) != cudaSuccess || cudaMalloc(&w, w_bytes) != cudaSuccess ||
+       cudaMalloc(&f, 64 * sizeof(float)) != cudaSuccess || cudaMalloc(&o, 4096) != cudaSuccess ||
+       cudaMalloc(&m, shape.nbeams * sizeof(int)) != cudaSuccess)
+        rc = fail(SW_ERR_CUDA, "allocation failed");
+    if(rc == SW_OK && (cudaMemsetAsync(v, 0, v_bytes, st) != cudaSuccess ||
+                       cudaMemsetAsync(w, 0, w_bytes, st) != cudaSuccess ||
+                       cudaMemsetAsync(f, 0, 64 * sizeof(float), st) != cudaSuccess ||
+                       cudaMemsetAsync(m, 0, shape.nbeams * sizeof(int), st) != cudaSuccess))
+        rc = fail(SW_ERR_CUDA, "memset failed");
+    if(rc == SW_OK) {
+        sw_cb_problem pr{};
+        pr.d_fpact = v;
+        pr.d_out = static_cast<int8_t*>(o);
+        pr.d_ib_raw = static_cast<const float*>(f);
+        pr.beam_start = 0;
+        pr.beam_count = shape.nbeams;
+        rc = swb::cb::launch(&shape, &pr, 1, w, static_cast<const float*>(f),
+                             static_cast<const float*>(f), static_cast<const int*>(m), nullptr,
+                             st, 1000ull * (unsigned long long)timeout_us, 1);
+    }
+    if(rc == SW_OK && cudaStreamSynchronize(st) != cudaSuccess)
+        rc = fail(SW_ERR_CUDA, cudaGetErrorString(cudaGetLastError()));
+    if(rc == SW_OK) {
+        int code = 0;
+        rc = sw_read_device_error(&code);
+        if(rc == SW_OK) {
+            sw_reset_device_error();
+            rc = code == swb::DEV_ERR_CB_TIMEOUT
+                     ? fail(SW_ERR_TIMEOUT, "the coherent beamformer's bounded wait timed out")
+                     : fail(SW_ERR_STATE, "no timeout recorded in the device error word");
+        }
+    }
+    cudaFree(v); cudaFree(w); cudaFree(f); cudaFree(o); cudaFree(m);
+    return rc;
 }
 
 }  // extern "C"

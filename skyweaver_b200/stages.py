@@ -27,6 +27,34 @@ def _stream(stream=None):
     return ctypes.c_void_p(s.cuda_stream)
 
 
+def device_error() -> int:
+    """The device error word that kernels with bounded waits set when a wait
+    gives up (0 = clean); it stays set until reset_device_error()."""
+    code = ctypes.c_int()
+    call("sw_read_device_error", ctypes.byref(code))
+    return code.value
+
+
+def reset_device_error() -> None:
+    call("sw_reset_device_error")
+
+
+def check_device_error() -> None:
+    """Raise SkyweaverError(SW_ERR_TIMEOUT) if a bounded device-side wait gave
+    up since the last reset, clearing the word."""
+    code = device_error()
+    if code:
+        reset_device_error()
+        raise _lib.SkyweaverError(_lib.SW_ERR_TIMEOUT,
+                                  f"a bounded device-side wait gave up (device error {code})")
+
+
+def cb_timeout_selftest(timeout_us: int = 20000, stream=None) -> int:
+    """Run the coherent beamformer's bounded-wait self-test; returns its
+    status (SW_ERR_TIMEOUT when the kernel timed out and returned)."""
+    return lib().sw_cb_timeout_selftest(int(timeout_us), _stream(stream))
+
+
 def channel_frequencies(centre, bandwidth, nchans):
     chbw = bandwidth / nchans
     return centre - bandwidth / 2.0 + chbw / 2.0 + chbw * np.arange(nchans)
@@ -369,6 +397,7 @@ class BeamformerPipeline:
         call("sw_pipeline_outputs", self.h, dm_idx, ctypes.byref(pcb), ctypes.byref(praw),
              ctypes.byref(pib), ctypes.byref(pst))
         torch.cuda.synchronize()
+        check_device_error()
         T = self.gulp // self.tscrunch
         S, F, B = self.nbeamsets, self.nchans, self.nbeams
         C = (4,) if self.stokes == "IQUV" else ()

@@ -207,6 +207,21 @@ def _report(out, ref):
     return "\n".join(lines)
 
 
+def test_coherent_beam_bounded_wait_times_out_and_context_survives(cuda, oracle):
+    """Every wait in the persistent beamformer is bounded.  The self-test
+    launches it with a copy producer that issues nothing, so the MMA role's
+    first wait can only end at its 20 ms deadline: the kernel must record
+    the timeout in the device error word, every role must leave, and the
+    context must stay usable (a normal launch afterwards is exact)."""
+    from skyweaver_b200 import _lib, stages
+    stages.reset_device_error()
+    assert stages.cb_timeout_selftest(20000) == _lib.SW_ERR_TIMEOUT
+    assert stages.device_error() == 0          # the self-test clears the word
+    out, ref, dbg, volts = _cb_case(cuda, oracle, 16, 128, 2, 1, 16, "I", True)
+    assert np.array_equal(dbg, volts) and np.array_equal(out, ref)
+    stages.check_device_error()                # nothing recorded by the normal launch
+
+
 @pytest.mark.parametrize("stokes", ["I", "Q", "U", "V", "IQUV"])
 @pytest.mark.parametrize("ib_sub", [True, False])
 def test_coherent_beam_stokes(cuda, oracle, stokes, ib_sub):
