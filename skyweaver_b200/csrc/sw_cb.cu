@@ -544,8 +544,8 @@ cb_kernel(const __grid_constant__ Params P)
         fence_before();
         __syncwarp();
         if(lane == 0) mbar_arrive(&acc_empty[grp]);
-        int ab = 0;
-        uint32_t aph = 0;
+        int ab = 0;        // accumulator buffer of the CTA's next tile
+        uint32_t aph = 0;  // phase parity of this group's buffer
         for(int item = blockIdx.x; item < P.nitems && !*s_abort; item += gridDim.x) {
             const Item it = decode(P, item);
             const Problem& pr = P.prob[it.p];
@@ -556,12 +556,15 @@ cb_kernel(const __grid_constant__ Params P)
             const float offs  = P.offset[bs * F + it.f];
             const int tile0 = it.tc * P.tpi;
             const int tile1 = min(ntiles_gulp, tile0 + P.tpi);
+            // tiles alternate between the buffers: this group takes every
+            // other tile, starting with the first one that lands in its buffer
+            const int first = tile0 + ((ab ^ grp) & 1);
             bool ok = true;
             constexpr int NC = STOKES == 4 ? 4 : 1;  // output components
             constexpr int kEmits = kSlice / TS;      // outputs per warp per tile
             // Output and IB-power elements of this warp's first output in
-            // tile0; both advance by kTileT / TS output samples per tile.
-            const int to0 = (tile0 * kTileT + h * kSlice) / TS;
+            // its first tile; both advance by 2 kTileT / TS output samples.
+            const int to0 = (first * kTileT + h * kSlice) / TS;
             int8_t* outp = pr.out + (((size_t)to0 * F + it.f) * P.nbeams + b) * NC;
             const float* ibq =
                 P.ib_subtract ? pr.ib_raw + (((size_t)bs * nout + to0) * F + it.f) * NC : nullptr;
@@ -571,118 +574,115 @@ cb_kernel(const __grid_constant__ Params P)
             // accumulator wait so that their latency hides behind it
             constexpr bool kPrefetch = kEmits * NC <= 4;
             float ibp[kPrefetch ? kEmits * NC : 1];
-            for(int tile = tile0; tile < tile1; ++tile) {
-                // tiles alternate between the buffers; the other group takes
-                // the tiles of the other buffer
-                if(ab == grp) {
-                    if constexpr(kPrefetch) {
-                        if(P.ib_subtract) {
+            for(int tile = first; tile < tile1; tile += 2) {
+                if constexpr(kPrefetch) {
+                    if(P.ib_subtract) {
 #pragma unroll
-                            for(int e = 0; e < kEmits; ++e) {
-                                if constexpr(NC == 1) {
-                                    ibp[e] = ibq[e * ib_emit];
-                                } else {
-                                    const float4 v = reinterpret_cast<const float4*>(ibq)[e * F];
-                                    ibp[4 * e] = v.x; ibp[4 * e + 1] = v.y;
-                                    ibp[4 * e + 2] = v.z; ibp[4 * e + 3] = v.w;
-                                }
+                        for(int e = 0; e < kEmits; ++e) {
+                            if constexpr(NC == 1) {
+                                ibp[e] = ibq[e * ib_emit];
+                            } else {
+                                const float4 v = reinterpret_cast<const float4*>(ibq)[e * F];
+                                ibp[4 * e] = v.x; ibp[4 * e + 1] = v.y;
+                                ibp[4 * e + 2] = v.z; ibp[4 * e + 3] = v.w;
                             }
                         }
                     }
-                    if(!mbar_wait(acc_full_s + 8 * ab, aph, s_abort, deadline, P.err)) { ok = false; break; }
-                    fence_after();
-                    float power[NC];  // carried across groups while tscrunch > 8
-#pragma unroll
-                    for(int c = 0; c < NC; ++c) power[c] = 0.0f;
-                    // One column group at a time: load, wait, reduce.  (Loading
-                    // the next group ahead of the arithmetic, or both groups at
-                    // once, was measured 1-2.5 % slower.)
-                    const uint32_t ta0 = lane_base + ab * 256 + h * kSlice;
-#pragma unroll
-                    for(int g = 0; g < kGroups; ++g) {
-                        uint32_t r0[kG], r1[kG], i0[kG], i1[kG];
-                        const uint32_t ta = ta0 + g * kG;
-                        if constexpr(kG == 16) {
-                            SW_TMEM_LD16(ta, r0);
-                            SW_TMEM_LD16(ta + 64, r1);
-                            SW_TMEM_LD16(ta + 128, i0);
-                            SW_TMEM_LD16(ta + 192, i1);
-                        } else {
-                            SW_TMEM_LD8(ta, r0);
-                            SW_TMEM_LD8(ta + 64, r1);
-                            SW_TMEM_LD8(ta + 128, i0);
-                            SW_TMEM_LD8(ta + 192, i1);
-                        }
-                        tmem_wait_ld();
-                        const int tbase = tile * kTileT + h * kSlice + g * kG;
-                        if(DBG && valid) {
-                            int2* dbg = reinterpret_cast<int2*>(P.debug);
-                            for(int t = 0; t < kG; ++t) {
-                                const size_t base_t = (size_t)it.f * P.nsamples + tbase + t;
-                                dbg[(base_t * 2 + 0) * P.nbeams + b] =
-                                    make_int2((int)r0[t], (int)i0[t]);
-                                dbg[(base_t * 2 + 1) * P.nbeams + b] =
-                                    make_int2((int)r1[t], (int)i1[t]);
-                            }
-                        }
-                        float st[NC][kG];
-                        if constexpr(STOKES == 4) stokes_iquv<kG>(r0, r1, i0, i1, st);
-                        else stokes_n<STOKES, kG>(r0, r1, i0, i1, st[0]);
-#pragma unroll
-                        for(int t = 0; t < kG; ++t) {
-#pragma unroll
-                            for(int c = 0; c < NC; ++c) power[c] = fadd(power[c], st[c][t]);
-                            const int u = g * kG + t;  // sample within this warp's slice
-                            const bool emit = ((u + 1) % TS) == 0;
-                            if(emit) {
-                                const int e = u / TS;  // emit index within the slice
-                                if constexpr(NC == 1) {
-                                    float v;
-                                    if(P.ib_subtract) {
-                                        const float ib = kPrefetch ? ibp[kPrefetch ? e : 0] : ibq[e * ib_emit];
-                                        v = rintf(fdiv(fsub(power[0], fmul(ib, 16129.0f)), scale));
-                                    } else if(STOKES == 0) {
-                                        v = rintf(fdiv(fsub(power[0], offs), scale));
-                                    } else {
-                                        v = rintf(fdiv(power[0], scale));
-                                    }
-                                    if(valid) outp[e * out_emit] = clamp_i8(v);
-                                } else {
-                                    // char4 {I, Q, U, V}; the IB power is float4
-                                    float v[4];
-                                    if(P.ib_subtract) {
-                                        const float4 ib = kPrefetch
-                                            ? make_float4(ibp[0], ibp[1], ibp[2], ibp[3])
-                                            : reinterpret_cast<const float4*>(ibq)[e * F];
-                                        v[0] = rintf(fdiv(fsub(power[0], fmul(ib.x, 16129.0f)), scale));
-                                        v[1] = rintf(fdiv(fsub(power[1], fmul(ib.y, 16129.0f)), scale));
-                                        v[2] = rintf(fdiv(fsub(power[2], fmul(ib.z, 16129.0f)), scale));
-                                        v[3] = rintf(fdiv(fsub(power[3], fmul(ib.w, 16129.0f)), scale));
-                                    } else {
-                                        v[0] = rintf(fdiv(fsub(power[0], offs), scale));
-                                        v[1] = rintf(fdiv(power[1], scale));
-                                        v[2] = rintf(fdiv(power[2], scale));
-                                        v[3] = rintf(fdiv(power[3], scale));
-                                    }
-                                    if(valid)
-                                        reinterpret_cast<char4*>(outp)[e * F * P.nbeams] =
-                                            make_char4(clamp_i8(v[0]), clamp_i8(v[1]),
-                                                       clamp_i8(v[2]), clamp_i8(v[3]));
-                                }
-#pragma unroll
-                                for(int c = 0; c < NC; ++c) power[c] = 0.0f;
-                            }
-                        }
-                    }
-                    fence_before();
-                    __syncwarp();
-                    if(lane == 0) mbar_arrive(&acc_empty[ab]);
                 }
-                if(++ab == 2) { ab = 0; aph ^= 1; }
-                outp += (kTileT / TS) * out_emit;
-                if(P.ib_subtract) ibq += (kTileT / TS) * ib_emit;
+                if(!mbar_wait(acc_full_s + 8 * grp, aph, s_abort, deadline, P.err)) { ok = false; break; }
+                fence_after();
+                float power[NC];  // carried across groups while tscrunch > 8
+#pragma unroll
+                for(int c = 0; c < NC; ++c) power[c] = 0.0f;
+                // One column group at a time: load, wait, reduce.  (Loading
+                // the next group ahead of the arithmetic, or both groups at
+                // once, was measured 1-2.5 % slower.)
+                const uint32_t ta0 = lane_base + grp * 256 + h * kSlice;
+#pragma unroll
+                for(int g = 0; g < kGroups; ++g) {
+                    uint32_t r0[kG], r1[kG], i0[kG], i1[kG];
+                    const uint32_t ta = ta0 + g * kG;
+                    if constexpr(kG == 16) {
+                        SW_TMEM_LD16(ta, r0);
+                        SW_TMEM_LD16(ta + 64, r1);
+                        SW_TMEM_LD16(ta + 128, i0);
+                        SW_TMEM_LD16(ta + 192, i1);
+                    } else {
+                        SW_TMEM_LD8(ta, r0);
+                        SW_TMEM_LD8(ta + 64, r1);
+                        SW_TMEM_LD8(ta + 128, i0);
+                        SW_TMEM_LD8(ta + 192, i1);
+                    }
+                    tmem_wait_ld();
+                    const int tbase = tile * kTileT + h * kSlice + g * kG;
+                    if(DBG && valid) {
+                        int2* dbg = reinterpret_cast<int2*>(P.debug);
+                        for(int t = 0; t < kG; ++t) {
+                            const size_t base_t = (size_t)it.f * P.nsamples + tbase + t;
+                            dbg[(base_t * 2 + 0) * P.nbeams + b] =
+                                make_int2((int)r0[t], (int)i0[t]);
+                            dbg[(base_t * 2 + 1) * P.nbeams + b] =
+                                make_int2((int)r1[t], (int)i1[t]);
+                        }
+                    }
+                    float st[NC][kG];
+                    if constexpr(STOKES == 4) stokes_iquv<kG>(r0, r1, i0, i1, st);
+                    else stokes_n<STOKES, kG>(r0, r1, i0, i1, st[0]);
+#pragma unroll
+                    for(int t = 0; t < kG; ++t) {
+#pragma unroll
+                        for(int c = 0; c < NC; ++c) power[c] = fadd(power[c], st[c][t]);
+                        const int u = g * kG + t;  // sample within this warp's slice
+                        const bool emit = ((u + 1) % TS) == 0;
+                        if(emit) {
+                            const int e = u / TS;  // emit index within the slice
+                            if constexpr(NC == 1) {
+                                float v;
+                                if(P.ib_subtract) {
+                                    const float ib = kPrefetch ? ibp[kPrefetch ? e : 0] : ibq[e * ib_emit];
+                                    v = rintf(fdiv(fsub(power[0], fmul(ib, 16129.0f)), scale));
+                                } else if(STOKES == 0) {
+                                    v = rintf(fdiv(fsub(power[0], offs), scale));
+                                } else {
+                                    v = rintf(fdiv(power[0], scale));
+                                }
+                                if(valid) outp[e * out_emit] = clamp_i8(v);
+                            } else {
+                                // char4 {I, Q, U, V}; the IB power is float4
+                                float v[4];
+                                if(P.ib_subtract) {
+                                    const float4 ib = kPrefetch
+                                        ? make_float4(ibp[0], ibp[1], ibp[2], ibp[3])
+                                        : reinterpret_cast<const float4*>(ibq)[e * F];
+                                    v[0] = rintf(fdiv(fsub(power[0], fmul(ib.x, 16129.0f)), scale));
+                                    v[1] = rintf(fdiv(fsub(power[1], fmul(ib.y, 16129.0f)), scale));
+                                    v[2] = rintf(fdiv(fsub(power[2], fmul(ib.z, 16129.0f)), scale));
+                                    v[3] = rintf(fdiv(fsub(power[3], fmul(ib.w, 16129.0f)), scale));
+                                } else {
+                                    v[0] = rintf(fdiv(fsub(power[0], offs), scale));
+                                    v[1] = rintf(fdiv(power[1], scale));
+                                    v[2] = rintf(fdiv(power[2], scale));
+                                    v[3] = rintf(fdiv(power[3], scale));
+                                }
+                                if(valid)
+                                    reinterpret_cast<char4*>(outp)[e * F * P.nbeams] =
+                                        make_char4(clamp_i8(v[0]), clamp_i8(v[1]),
+                                                   clamp_i8(v[2]), clamp_i8(v[3]));
+                            }
+#pragma unroll
+                            for(int c = 0; c < NC; ++c) power[c] = 0.0f;
+                        }
+                    }
+                }
+                fence_before();
+                __syncwarp();
+                if(lane == 0) mbar_arrive(&acc_empty[grp]);
+                aph ^= 1;
+                outp += (2 * kTileT / TS) * out_emit;
+                if(P.ib_subtract) ibq += (2 * kTileT / TS) * ib_emit;
             }
             if(!ok) break;
+            ab ^= (tile1 - tile0) & 1;
         }
     }
     fence_before();
