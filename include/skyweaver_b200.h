@@ -206,7 +206,7 @@ typedef struct sw_cb_shape {
     int ib_subtract;    /* SKYWEAVER_IB_SUBTRACTION (default 1)           */
     size_t row_stride;  /* FPACT row stride (samples)                     */
     size_t sample_offset;
-    int tiles_per_item; /* 64-sample tiles per work item (0: 16; see sw_autotune) */
+    int tiles_per_item; /* 64-sample tiles per work item (0: 64; see sw_autotune) */
 } sw_cb_shape;
 
 /* Replaces CoherentBeamformer<BfTraits>::beamform

@@ -163,7 +163,7 @@ extern "C" int sw_autotune(int nantennas, int nbeams, int nchans, int nsamples, 
         SW_CUDA_CHECK(cudaStreamSynchronize(s));
     }
     best.cb_ms = 1e30f;
-    for(int tpi : {4, 8, 16, 32, 64}) {
+    for(int tpi : {4, 8, 16, 32, 64, 128}) {
         if(tpi > T / 64 && tpi != 4) break;
         sw_cb_shape shape{F, T, A, nbeams, ts, 0, 1, (size_t)T, 0, tpi};
         std::vector<sw_cb_problem> probs;

@@ -41,7 +41,7 @@ constexpr int kTileT       = 64;   // samples per tile
 constexpr int kN           = 2 * kTileT;
 constexpr int kVStages     = 4;
 constexpr int kWStages     = 2;
-constexpr int kTilesPerItem = 16;  // default work item: 1024 samples of one channel
+constexpr int kTilesPerItem = 64;  // default work item: 4096 samples of one channel
 constexpr int kMaxDm       = 16;
 constexpr int kMaxProblems = 96;
 // Epilogue warps: two groups of 8, one per accumulator buffer, so that each

@@ -238,7 +238,7 @@ def test_autotune_choices_and_results(cuda, oracle):
     dms = [0.0, 150.0]
     t = stages.autotune(A, B, F, T, ts, dms, centre, bw)
     assert t["fft_len"] > t["overlap"] and t["fft_len"] & (t["fft_len"] - 1) == 0
-    assert t["cb_tiles_per_item"] in (4, 8, 16, 32, 64)
+    assert t["cb_tiles_per_item"] in (4, 8, 16, 32, 64, 128)
     assert t["cdd_ms"] > 0 and t["cb_ms"] > 0
     t0 = time.perf_counter()
     assert stages.autotune(A, B, F, T, ts, dms, centre, bw) == t      # cached
