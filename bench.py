@@ -14,6 +14,10 @@ value  = real-time factor of the batched, graph-captured pipeline with the
          over ranks; every rank processes its own subband: weak scaling).
 e2e    = the same through the public host API (pinned TAFTP H2D and the D2H
          of every DM's coherent-beam output inside the timed region).
+Secondary lines in the same JSON object: the plain (eager, per-DM) pipeline,
+the per-kernel breakdown, ragged beamsets (8 beamsets x 4 DMs, grouped vs
+plain), long_fft (256 beams with 65536-point dedispersion windows) and uhf
+(UHF band, 2048 beams, device incoherent dedispersion of 128 trial DMs).
 
 python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 """
@@ -281,6 +285,9 @@ def main_b200(args):
     # ---- ragged (DM x beamset) problems: grouped vs plain
     ragged = ragged_case(torch, stages, synthetic, args.steps)
 
+    # ---- 65536-point dedispersion windows, 256 beams (precision configuration)
+    long_fft = long_fft_case(torch, stages, synthetic, taftp, common, args.steps)
+
     # ---- end to end through the host API (pinned H2D + D2H inside the timing)
     h_in = torch.empty(taftp.shape, dtype=torch.int8, pin_memory=True)
     h_in.copy_(taftp)
@@ -327,6 +334,7 @@ def main_b200(args):
             "kernels": kern, "roofline": roof, "hbm_peak_gbs": hbm_peak, "e2e": e2e,
             "gpu_launches": launches * args.steps, "clocks": clocks}
     pipe.close()
+    line["long_fft"] = long_fft
     if not args.no_uhf:
         free, _ = torch.cuda.mem_get_info()
         if free >= 120e9:   # the UHF chain holds ~100 GB (aggregation buffers included)
@@ -405,6 +413,36 @@ def kernel_breakdown(torch, stages, taftp, delays, fft_len, overlap, centre, bwi
 
 RAGGED = dict(nant=64, nchans=64, gulp=32768, tscrunch=16, dms=[0.0, 50.0, 150.0, 500.0],
               ants=[64, 57, 48, 40, 32, 24, 16, 8], beams=[512, 256, 256, 128, 128, 64, 64, 32])
+
+
+def long_fft_case(torch, stages, synthetic, taftp, common, K):
+    """The benchmark gulp with 256 beams and 65536-point overlap-save
+    windows (the precision configuration: one window per channel and gulp,
+    four-step split FFT through a workspace), DMs {0, 50, 150, 500}; graph +
+    grouped beamformer, input resident in HBM.  Its precision against the FP64
+    oracle and the DM-150 pulse are checked by the GPU tests."""
+    B = 256
+    cfg = dict(common, nbeams=B, beamset_mapping=np.zeros(B, np.int32))
+    pipe = stages.BeamformerPipeline(**cfg, fft_len=65536, grouped=True, use_graph=True)
+    pipe.set_delays(synthetic.delay_model(synthetic.rng(256), B, cfg["nantennas"]), 1.7e9)
+    fft_len, overlap = pipe.fft_plan()
+    gulp_s = cfg["gulp_samples"] * tsamp()
+    for i in range(3):
+        pipe.process_device(taftp, 1.7e9 + i * gulp_s)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for i in range(K):
+        pipe.process_device(taftp, 1.7e9 + (3 + i) * gulp_s)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / K
+    pipe.close()
+    return {"workload": f"{cfg['nantennas']}ant x {B}beam x {cfg['nchans']}ch x "
+                        f"{cfg['gulp_samples']}-sample gulps, DMs {list(cfg['dms'])}, "
+                        f"{fft_len}-point windows (overlap {overlap})",
+            "fft_len": fft_len, "overlap": overlap, "ms_per_gulp": ms,
+            "rtf": gulp_s / (ms * 1e-3), "timed_gulps": K, "warmup_gulps": 3}
 
 
 def ragged_case(torch, stages, synthetic, K):
