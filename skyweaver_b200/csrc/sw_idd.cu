@@ -6,21 +6,16 @@
 //                       / scale_factor),   t = max_delay + t' * ts
 // with truncation toward zero (types.cuh:211-221).  The int8 sums are exact
 // integers (the reference accumulates them in float, exact below 2^24), so
-// the kernel sums bytes with SWAR arithmetic: each 32-bit word of 4 beams is
-// biased to unsigned (x + 128) and split into two pairs of 16-bit lanes,
-// flushed into 32-bit accumulators every 256 additions.  The final
-// float divide is the reference's single IEEE division.
+// the kernels sum bytes in int32: beam b of a 32-bit word of 4 beams is added
+// by dp4a(word, 1 << 8b, acc), one instruction per addition on the integer
+// multiply-add pipe.  (Biasing each word to unsigned and adding pairs of
+// 16-bit lanes, two per instruction, measured 8 % slower: it needs a xor and
+// two byte permutes per word on the pipe that also issues the adds.)  The
+// final float divide is the reference's single IEEE division.
 #include "sw_common.cuh"
 
 namespace swb {
 namespace {
-
-__device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel)
-{
-    uint32_t d;
-    asm("prmt.b32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(sel));
-    return d;
-}
 
 // One CTA = (trial DM, output sample, block of 128 beam quads).  The linear
 // block index runs over the DMs of a group of `group` DMs fastest, then
@@ -46,30 +41,19 @@ idd_k(const uint32_t* __restrict__ tfb, int nchans, int nquads,
     const int t = max_delay + to * tscrunch;
     const int* dl_f = delays + (size_t)d * nchans;
     int acc[4] = {0, 0, 0, 0};
-    uint32_t lo = 0, hi = 0;
-    int pending = 0;
     for(int tau = 0; tau < tscrunch; ++tau) {
 #pragma unroll 4
         for(int f = 0; f < nchans; ++f) {
             const size_t row = (size_t)(t + tau - dl_f[f]) * nchans + f;
-            const uint32_t w = tfb[row * nquads + q] ^ 0x80808080u;
-            lo += prmt(w, 0, 0x4240);  // bytes 0,2 -> 16-bit lanes
-            hi += prmt(w, 0, 0x4341);  // bytes 1,3
-            if(++pending == 256) {
-                acc[0] += (int)(lo & 0xffff); acc[2] += (int)(lo >> 16);
-                acc[1] += (int)(hi & 0xffff); acc[3] += (int)(hi >> 16);
-                lo = hi = 0;
-                pending = 0;
-            }
+            const int w = (int)tfb[row * nquads + q];
+#pragma unroll
+            for(int b = 0; b < 4; ++b) acc[b] = __dp4a(w, 1 << (8 * b), acc[b]);
         }
     }
-    acc[0] += (int)(lo & 0xffff); acc[2] += (int)(lo >> 16);
-    acc[1] += (int)(hi & 0xffff); acc[3] += (int)(hi >> 16);
-    const int bias = 128 * tscrunch * nchans;
     uint32_t packed = 0;
 #pragma unroll
     for(int k = 0; k < 4; ++k) {
-        const float v = fdiv((float)(acc[k] - bias), scale_factor);
+        const float v = fdiv((float)acc[k], scale_factor);
         packed |= ((uint32_t)(uint8_t)clamp_i8(v)) << (8 * k);
     }
     tdb[((size_t)to * ndms + d) * nquads + q] = packed;
@@ -118,36 +102,22 @@ idd16_k(const uint4* __restrict__ tfb, int nchans, int nq16,
     for(int k = 0; k < 16 * V; ++k) acc[k] = 0;
     for(int tau = 0; tau < tscrunch; ++tau) {
         const uint4* bt = tfb + (long long)(t + tau) * row + q;
-        for(int f0 = 0; f0 < nchans; f0 += 256) {
-            const int f1 = min(nchans, f0 + 256);
-            uint32_t lo[4 * V], hi[4 * V];
-#pragma unroll
-            for(int k = 0; k < 4 * V; ++k) lo[k] = hi[k] = 0;
 #pragma unroll 4
-            for(int f = f0; f < f1; ++f) {
-                const uint4* p = bt + s_off[f];
+        for(int f = 0; f < nchans; ++f) {
+            const uint4* p = bt + s_off[f];
 #pragma unroll
-                for(int u = 0; u < V; ++u) {
-                    const uint4 v = p[u];
-                    const uint32_t w[4] = {v.x ^ 0x80808080u, v.y ^ 0x80808080u,
-                                           v.z ^ 0x80808080u, v.w ^ 0x80808080u};
+            for(int u = 0; u < V; ++u) {
+                const uint4 v = p[u];
+                const int w[4] = {(int)v.x, (int)v.y, (int)v.z, (int)v.w};
 #pragma unroll
-                    for(int k = 0; k < 4; ++k) {
-                        lo[4 * u + k] += prmt(w[k], 0, 0x4240);  // bytes 0,2 -> 16-bit lanes
-                        hi[4 * u + k] += prmt(w[k], 0, 0x4341);  // bytes 1,3
-                    }
-                }
-            }
+                for(int k = 0; k < 4; ++k)
 #pragma unroll
-            for(int k = 0; k < 4 * V; ++k) {  // at most 256 adds of <= 255 per lane
-                acc[4 * k + 0] += (int)(lo[k] & 0xffff);
-                acc[4 * k + 2] += (int)(lo[k] >> 16);
-                acc[4 * k + 1] += (int)(hi[k] & 0xffff);
-                acc[4 * k + 3] += (int)(hi[k] >> 16);
+                    for(int b = 0; b < 4; ++b)
+                        acc[16 * u + 4 * k + b] =
+                            __dp4a(w[k], 1 << (8 * b), acc[16 * u + 4 * k + b]);
             }
         }
     }
-    const int bias = 128 * tscrunch * nchans;
 #pragma unroll
     for(int u = 0; u < V; ++u) {
         uint32_t packed[4];
@@ -156,7 +126,7 @@ idd16_k(const uint4* __restrict__ tfb, int nchans, int nq16,
             packed[k] = 0;
 #pragma unroll
             for(int b = 0; b < 4; ++b) {
-                const float v = fdiv((float)(acc[16 * u + 4 * k + b] - bias), scale_factor);
+                const float v = fdiv((float)acc[16 * u + 4 * k + b], scale_factor);
                 packed[k] |= ((uint32_t)(uint8_t)clamp_i8(v)) << (8 * b);
             }
         }
