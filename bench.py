@@ -602,10 +602,31 @@ def uhf_case(torch, stages, synthetic, K, W):
 def profile_case(which, nchans=16, reps=3):
     """Small single-kernel case for ncu captures: `nchans` channels of the
     benchmark workload (268 MB of voltages for 16 channels, above L2), one
-    warm-up launch and `reps` profiled launches of one kernel."""
+    warm-up launch and `reps` profiled launches of one kernel.  `idd`: the
+    UHF incoherent-dedispersion trials (128 DMs over 0-100, 256 channels,
+    2048 beams) on 4096 output samples, a 5.9 GB beam buffer."""
     import torch
 
     from skyweaver_b200 import stages, synthetic
+    if which == "idd":
+        U = UHF
+        F, B, D = U["nchans"], U["nbeams"], 4096
+        freqs = U["top"] - F * U["chbw"] + U["chbw"] * (np.arange(F) + 0.5)
+        cb_tsamp = U["tscrunch"] / U["chbw"]
+        trials = np.linspace(0.0, 2 * U["trial_span"], U["ntrials"]).astype(np.float32)
+        k = 4.148806423e15
+        dl = np.array([[int(k * (1 / freqs[0] ** 2 - 1 / f ** 2) * d / cb_tsamp + 0.5)
+                        for f in freqs] for d in trials], np.int32)
+        maxd = int(dl.max())
+        tfb = torch.randint(-128, 128, (D + maxd, F, B), dtype=torch.int8, device="cuda")
+        delays = torch.from_numpy(dl).cuda()
+        sf = float(np.float32(math.sqrt(F)))
+        fn = lambda: stages.incoherent_dedisperse(tfb, delays, maxd, 1, sf)
+        for _ in range(1 + reps):
+            fn()
+        torch.cuda.synchronize()
+        print(f"profile case idd: {U['ntrials']} DMs, {D} samples, {1 + reps} launches ok")
+        return
     A, B, T, ts = WORK["nant"], WORK["nbeams"], WORK["gulp"], WORK["tscrunch"]
     F = nchans
     dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
@@ -639,7 +660,7 @@ def profile_case(which, nchans=16, reps=3):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--profile", choices=["cb", "cdd"], default=None,
+    ap.add_argument("--profile", choices=["cb", "cdd", "idd"], default=None,
                     help="run a small single-kernel case for ncu and exit")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
