@@ -25,7 +25,8 @@
 //               lane quarter, 32 samples of the tile apiece
 // TMEM: 512 columns = 2 accumulator buffers x (D_re 128 | D_im 128).
 // Every wait is bounded by a kernel-wide deadline; on expiry the CTA records
-// DEV_ERR_CB_TIMEOUT in the device error word, stops issuing work and exits cleanly.
+// DEV_ERR_CB_TIMEOUT in the device error word, stops issuing work, waits
+// (bounded) for the copies and MMAs it has in flight and exits.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
