@@ -361,6 +361,19 @@ static void dada_io_tests(const std::string& scratch)
     std::puts("PASS dada_io");
 }
 
+// The coherent beamformer's bounded waits, through the C ABI: a launch whose
+// copy producer never issues must report SW_ERR_TIMEOUT and leave the device
+// error word clear, and the context must stay usable.
+static void bounded_wait_test()
+{
+    EXPECT(sw_reset_device_error() == SW_OK);
+    EXPECT(sw_cb_timeout_selftest(20000, nullptr) == SW_ERR_TIMEOUT);
+    int code = -1;
+    EXPECT(sw_read_device_error(&code) == SW_OK && code == 0);
+    EXPECT(sw_cb_timeout_selftest(0, nullptr) == SW_ERR_INVALID);
+    std::puts("PASS bounded_wait");
+}
+
 int main(int argc, char** argv)
 {
     const std::string golden = argc > 1 ? argv[1] : "tests/golden";
@@ -374,6 +387,8 @@ int main(int argc, char** argv)
     pipeline_smoke(golden);
     idd_pipeline_tests();
     dada_io_tests(argc > 2 ? argv[2] : ".");
+    bounded_wait_test();
+    beamformer_tests();  // the context is still usable after the timeout
     std::puts("ALL PASS");
     return 0;
 }
