@@ -141,13 +141,58 @@ def run_reference(args):
 
 # ---------------------------------------------------------------- clocks
 class Clocks:
+    """SM clock, power and clock-event reasons sampled while the timed region
+    runs: NVML every 10 ms from a thread (nvidia-smi -lms 200 if NVML is not
+    importable).  summary() gives the median SM clock under load, the max
+    clock and every slowdown reason seen."""
+
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+
     def __init__(self, index):
         self.index = index
-        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.rows = []          # (sm_mhz, max_mhz, watts, reasons set)
+        self.stop = threading.Event()
+        self.thread = None
         self.p = None
+        self.f = None
+
+    def _nvml_handle(self, nv):
+        try:
+            import torch
+            pr = torch.cuda.get_device_properties(self.index)
+            bus = f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+            return nv.nvmlDeviceGetHandleByPciBusId(bus.encode())
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(self.index)
+
+    def _sample(self, nv, h):
+        bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while not self.stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                w = nv.nvmlDeviceGetPowerUsage(h) / 1000.0
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.rows.append((float(sm), float(mx), w, {n for n, b in bits.items() if r & b}))
+            except Exception:
+                pass
+            self.stop.wait(0.01)
 
     def __enter__(self):
         try:
+            import pynvml as nv
+            nv.nvmlInit()
+            h = self._nvml_handle(nv)
+            self.thread = threading.Thread(target=self._sample, args=(nv, h), daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.thread = None
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             self.p = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index),
                  "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -160,29 +205,36 @@ class Clocks:
         return self
 
     def __exit__(self, *a):
+        if self.thread:
+            self.stop.set()
+            self.thread.join()
         if self.p:
             self.p.terminate()
             self.p.wait()
 
     def summary(self):
-        self.f.flush()
-        self.f.seek(0)
-        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
-        sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in rows:
-            try:
-                sm.append(float(r[0]))
-                mx.append(float(r[1]))
-                for nm, v in zip(names, r[4:8]):
-                    if v.strip().lower() == "active":
-                        reasons.add(nm)
-            except (ValueError, IndexError):
-                pass
-        if not sm:
+        rows = list(self.rows)
+        if self.f is not None:
+            self.f.flush()
+            self.f.seek(0)
+            for r in (r.split(",") for r in self.f.read().strip().splitlines() if r.strip()):
+                try:
+                    rows.append((float(r[0]), float(r[1]), float(r[2]),
+                                 {n for n, v in zip(self.NAMES, r[4:8])
+                                  if v.strip().lower() == "active"}))
+                except (ValueError, IndexError):
+                    pass
+        if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)),
-                "reasons": sorted(reasons), "samples": len(sm)}
+        # the median under load: samples drawing more than half the peak power
+        wmax = max(r[2] for r in rows)
+        load = [r for r in rows if r[2] >= 0.5 * wmax] or rows
+        return {"sm_mhz": float(np.median([r[0] for r in load])),
+                "sm_max_mhz": float(max(r[1] for r in rows)),
+                "reasons": sorted(set().union(*(r[3] for r in rows))),
+                "samples": len(rows), "samples_under_load": len(load),
+                "power_w_median": float(np.median([r[2] for r in load])),
+                "source": "nvml 10 ms" if self.thread else "nvidia-smi 200 ms"}
 
 
 # ------------------------------------------------------- rank decomposition
