@@ -157,16 +157,17 @@ def incoherent_beamform(fpact, nsamples, tscrunch, scale, offset, beamset_weight
 
 
 def cb_shape(fpact, nsamples, nbeams, tscrunch, stokes="I", ib_subtract=True,
-             offset_samples=0):
+             offset_samples=0, tiles_per_item=0):
     F, P, A, _, stride = fpact.shape
     return CbShape(F, nsamples, A, nbeams, tscrunch, STOKES[stokes], int(ib_subtract),
-                   stride, offset_samples)
+                   stride, offset_samples, tiles_per_item)
 
 
 def coherent_beamform(fpact, weights_gemm, scale, offset, mapping, ib_raw, nsamples,
                       tscrunch, stokes="I", ib_subtract=True, beam_start=0, beam_count=None,
-                      out=None, debug=False, offset_samples=0, stream=None):
-    """CoherentBeamformer::beamform (plain: one problem) -> int8 TFB."""
+                      out=None, debug=False, offset_samples=0, tiles_per_item=0, stream=None):
+    """CoherentBeamformer::beamform (plain: one problem) -> int8 TFB.
+    tiles_per_item: 64-sample tiles per work item (0: the library default)."""
     F = fpact.shape[0]
     nbeams = weights_gemm.shape[2]
     beam_count = nbeams if beam_count is None else beam_count
@@ -175,7 +176,8 @@ def coherent_beamform(fpact, weights_gemm, scale, offset, mapping, ib_raw, nsamp
                           dtype=torch.int8, device=fpact.device)
     dbg = (torch.zeros((F, nsamples, 2, nbeams, 2), dtype=torch.int32, device=fpact.device)
            if debug else None)
-    shape = cb_shape(fpact, nsamples, nbeams, tscrunch, stokes, ib_subtract, offset_samples)
+    shape = cb_shape(fpact, nsamples, nbeams, tscrunch, stokes, ib_subtract, offset_samples,
+                     tiles_per_item)
     prob = CbProblem(fpact.data_ptr(), out.data_ptr(),
                      ib_raw.data_ptr() if ib_raw is not None else None, beam_start, beam_count)
     call("sw_coherent_beamform", ctypes.byref(shape), ctypes.byref(prob), _ptr(weights_gemm),
@@ -185,11 +187,12 @@ def coherent_beamform(fpact, weights_gemm, scale, offset, mapping, ib_raw, nsamp
 
 def coherent_beamform_grouped(problems, weights_gemm, scale, offset, mapping, nsamples,
                               tscrunch, stokes="I", ib_subtract=True, offset_samples=0,
-                              stream=None):
+                              tiles_per_item=0, stream=None):
     """problems: list of (fpact, out, ib_raw, beam_start, beam_count)."""
     fp0 = problems[0][0]
     nbeams = weights_gemm.shape[2]
-    shape = cb_shape(fp0, nsamples, nbeams, tscrunch, stokes, ib_subtract, offset_samples)
+    shape = cb_shape(fp0, nsamples, nbeams, tscrunch, stokes, ib_subtract, offset_samples,
+                     tiles_per_item)
     arr = (CbProblem * len(problems))(*[
         CbProblem(p[0].data_ptr(), p[1].data_ptr(), p[2].data_ptr() if p[2] is not None else None,
                   p[3], p[4]) for p in problems])

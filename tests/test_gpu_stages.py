@@ -207,6 +207,40 @@ def _report(out, ref):
     return "\n".join(lines)
 
 
+@pytest.mark.parametrize("tpi", [1, 3, 5, 7, 64, 1024])
+def test_coherent_beam_work_item_sizes(cuda, oracle, tpi):
+    """The persistent beamformer splits each (problem, channel, 128-beam
+    block) into work items of `tpi` 64-sample tiles, and its two epilogue
+    groups take alternate tiles across item boundaries: odd item lengths
+    (and items cut short at the end of the gulp) must give the same bytes."""
+    from skyweaver_b200 import stages, synthetic
+    A, F, B, H, ts = 32, 3, 256, 7, 16          # 1792 samples = 28 tiles
+    g = synthetic.rng(40 + tpi)
+    taftp = synthetic.voltages_taftp(g, H, A, F, sigma=32)
+    T = H * 256
+    ftpa = oracle.transpose(taftp, A)
+    th = g.uniform(0, 2 * np.pi, size=(F, B, A))
+    w = np.stack([np.rint(127 * np.cos(th)), np.rint(127 * np.sin(th))], -1).astype(np.int8)
+    level = 32.0
+    cb_s = (127 * level * math.sqrt(A)) ** 2
+    dof = 2 * ts * 2
+    scales = np.full(F, cb_s * math.sqrt(2 * dof) / level, np.float32)
+    offsets = np.full(F, cb_s * dof, np.float32)
+    bw = np.ones((1, A), np.float32)
+    mapping = np.zeros(B, np.int32)
+    ib_dof = 2 * ts * A * 2
+    ib_scale = np.full(F, level ** 2 * math.sqrt(2 * ib_dof) / level, np.float32)
+    ib_off = np.full(F, level ** 2 * ib_dof, np.float32)
+    fp = stages.transpose_fpact(_dev(cuda, taftp), A)
+    raw_ib, _ = stages.incoherent_beamform(fp, T, ts, _dev(cuda, ib_scale), _dev(cuda, ib_off),
+                                           _dev(cuda, bw))
+    gemm = stages.pack_weights(_dev(cuda, w))
+    out = stages.coherent_beamform(fp, gemm, _dev(cuda, scales), _dev(cuda, offsets),
+                                   _dev(cuda, mapping), raw_ib, T, ts, tiles_per_item=tpi)
+    ref = oracle.coherent_beam(ftpa, w, ts, scales, offsets, bw, mapping)
+    assert np.array_equal(_np(out), ref), _report(_np(out), ref)
+
+
 def test_coherent_beam_bounded_wait_times_out_and_context_survives(cuda, oracle):
     """Every wait in the persistent beamformer is bounded.  The self-test
     launches it with a copy producer that issues nothing, so the MMA role's
