@@ -85,11 +85,35 @@ ib_k(IbArgs args, int bs0)
     }
 
     const bool words = (args.tscrunch % 4) == 0;
+    // 16-byte loads when each thread's samples are whole aligned 16-byte runs
+    const bool quads = (args.tscrunch % 16) == 0 && (args.row_stride % 16) == 0 &&
+                       (args.offset % 16) == 0 &&
+                       (reinterpret_cast<uintptr_t>(args.fpact) & 15) == 0;
     for(int a = 0; a < args.nant; ++a) {
         const uint8_t* r0 = args.fpact + (((size_t)f * P + 0) * args.nant + a) * 2 * args.row_stride + args.offset + t0;
         const uint8_t* r1 = args.fpact + (((size_t)f * P + 1) * args.nant + a) * 2 * args.row_stride + args.offset + t0;
         int pI = 0, pQ = 0, pU = 0, pV = 0;
-        if(words) {
+        if(quads) {
+            for(int k = 0; k < args.tscrunch; k += 16) {
+                const uint4 R0 = *reinterpret_cast<const uint4*>(r0 + k);
+                const uint4 I0 = *reinterpret_cast<const uint4*>(r0 + args.row_stride + k);
+                const uint4 R1 = *reinterpret_cast<const uint4*>(r1 + k);
+                const uint4 I1 = *reinterpret_cast<const uint4*>(r1 + args.row_stride + k);
+                const int xr0[4] = {(int)R0.x, (int)R0.y, (int)R0.z, (int)R0.w};
+                const int xi0[4] = {(int)I0.x, (int)I0.y, (int)I0.z, (int)I0.w};
+                const int xr1[4] = {(int)R1.x, (int)R1.y, (int)R1.z, (int)R1.w};
+                const int xi1[4] = {(int)I1.x, (int)I1.y, (int)I1.z, (int)I1.w};
+#pragma unroll
+                for(int q = 0; q < 4; ++q) {
+                    const int e0 = __dp4a(xi0[q], xi0[q], __dp4a(xr0[q], xr0[q], 0));
+                    const int e1 = __dp4a(xi1[q], xi1[q], __dp4a(xr1[q], xr1[q], 0));
+                    pI += e0 + e1;
+                    pQ += e0 - e1;
+                    pU += __dp4a(xi0[q], xi1[q], __dp4a(xr0[q], xr1[q], 0));
+                    pV += __dp4a(xi0[q], xr1[q], 0) - __dp4a(xr0[q], xi1[q], 0);
+                }
+            }
+        } else if(words) {
             for(int k = 0; k < args.tscrunch; k += 4) {
                 const int xr0 = *reinterpret_cast<const int*>(r0 + k);
                 const int xi0 = *reinterpret_cast<const int*>(r0 + args.row_stride + k);

@@ -23,18 +23,24 @@ namespace {
 constexpr int kStatsThreads = 256;
 constexpr int kChunkSamples = 16384;  // samples per CTA per row pair
 
-__device__ __forceinline__ void accum_word(uint32_t w, int& s1, int& s2,
-                                           long long& s3, long long& s4)
+// S1 and S2 by dp4a; the cubes (|x^3| <= 2^21) go into a 32-bit partial
+// that the caller widens once per 16-byte load, and the four fourth powers of
+// a word (x^4 <= 2^28, four of them < 2^31) are summed in 32 bits before one
+// 64-bit add.
+__device__ __forceinline__ void accum_word(uint32_t w, int& s1, int& s2, int& s3w,
+                                           long long& s4)
 {
     s1 = __dp4a((int)w, 0x01010101, s1);
     s2 = __dp4a((int)w, (int)w, s2);
+    int q4 = 0;
 #pragma unroll
     for(int k = 0; k < 4; ++k) {
         const int x  = (int)(int8_t)(w >> (8 * k));
         const int x2 = x * x;
-        s3 += (long long)(x2 * x);
-        s4 += (long long)x2 * x2;
+        s3w += x2 * x;
+        q4 += x2 * x2;
     }
+    s4 += q4;
 }
 
 // grid: (chunks per series, F*P*A series).  Each series is the pair of
@@ -53,10 +59,12 @@ stats_partial_k(const uint8_t* __restrict__ fpact, size_t row_stride,
         const uint8_t* row = fpact + (series * 2 + c) * row_stride + sample_offset;
         for(int t = t0 + threadIdx.x * 16; t < t1; t += kStatsThreads * 16) {
             const uint4 v = *reinterpret_cast<const uint4*>(row + t);
-            accum_word(v.x, s1, s2, s3, s4);
-            accum_word(v.y, s1, s2, s3, s4);
-            accum_word(v.z, s1, s2, s3, s4);
-            accum_word(v.w, s1, s2, s3, s4);
+            int s3w = 0;  // 16 cubes: |sum| <= 2^25
+            accum_word(v.x, s1, s2, s3w, s4);
+            accum_word(v.y, s1, s2, s3w, s4);
+            accum_word(v.z, s1, s2, s3w, s4);
+            accum_word(v.w, s1, s2, s3w, s4);
+            s3 += s3w;
         }
     }
     long long v1 = s1, v2 = s2, v3 = s3, v4 = s4;
