@@ -79,6 +79,41 @@ class DeviceBuffer {
     std::size_t _n = 0;
 };
 
+// --------------------------------------------------------------- Description
+// The metadata that the reference's DescribedVector carries beside its data
+// (cpp/skyweaver/DescribedVector.hpp:96-573: dimension order and extents,
+// channel frequencies, tsamp, utc_offset, dms, reference_dm).  Here the data
+// stays a plain device buffer and its description travels beside it, with
+// the reference's getter names.
+struct Description {
+    std::string dims;                  // dimension order, outermost first ("TFB", "BTF", ...)
+    std::vector<std::size_t> sizes;    // extent of each dimension in `dims`
+    std::vector<double> freqs;         // channel centre frequencies (Hz)
+    double sample_period = 0.0;        // seconds per sample of the T dimension
+    double offset = 0.0;               // seconds: the dedisperser's filter delay
+    std::vector<float> trial_dms;      // DMs of a D dimension
+    float coherent_dm = 0.0f;          // DM the voltages were coherently dedispersed to
+
+    const std::vector<std::size_t>& extents() const { return sizes; }
+    std::string dims_as_string() const { return dims; }
+    const std::vector<double>& frequencies() const { return freqs; }
+    double tsamp() const { return sample_period; }
+    double utc_offset() const { return offset; }
+    const std::vector<float>& dms() const { return trial_dms; }
+    float reference_dm() const { return coherent_dm; }
+    std::size_t extent(char d) const
+    {
+        std::size_t n = 1;
+        for(std::size_t i = 0; i < dims.size(); ++i)
+            if(dims[i] == d) n *= sizes[i];
+        return n;
+    }
+    std::size_t nsamples() const { return extent('T'); }
+    std::size_t nchannels() const { return extent('F'); }
+    std::size_t nbeams() const { return extent('B'); }
+    std::size_t ndms() const { return extent('D'); }
+};
+
 // --------------------------------------------------------- DedispersionPlan
 // cpp/skyweaver/DedispersionPlan.hpp:11-123, src/DedispersionPlan.cpp:17-78
 struct DedispersionPlanBlock {
@@ -795,6 +830,32 @@ class BeamformerPipeline {
         _out.resize(sw_pipeline_cb_bytes_per_dm(_p) * c.ndms);
     }
     ~BeamformerPipeline() { sw_pipeline_destroy(_p); }
+
+    // The description of one coherent DM's beams, as the reference's CB
+    // handler finds it on its TFBPowersD (CoherentBeamformer.cu:231-235,
+    // CoherentDedisperser.cu:224, detail/BeamformerPipeline.cu:191-193):
+    // TFB (element char4 for IQUV), tsamp = cb_tscrunch x channel sample,
+    // utc_offset = the dedisperser's filter delay, reference_dm = the DM.
+    Description describe_cb(std::size_t dm_idx) const
+    {
+        Description d = describe_base(dm_idx);
+        d.dims  = "TFB";
+        d.sizes = {_config.gulp_length_samps() / _config.cb_tscrunch(), _config.nchans(),
+                   _config.nbeams()};
+        d.sample_period *= (double)_config.cb_tscrunch();
+        return d;
+    }
+    // The incoherent beam of the same DM: BTF over beamsets (float raw power
+    // and int8), tsamp = ib_tscrunch x channel sample.
+    Description describe_ib(std::size_t dm_idx) const
+    {
+        Description d = describe_base(dm_idx);
+        d.dims  = "BTF";
+        d.sizes = {(std::size_t)_delays.nbeamsets(),
+                   _config.gulp_length_samps() / _config.ib_tscrunch(), _config.nchans()};
+        d.sample_period *= (double)_config.ib_tscrunch();
+        return d;
+    }
     // one gulp of TAFTP voltages already in device memory; each DM's
     // coherent beams stay on the device and go to
     // handler(d_tfb, nsamples, dm_idx, stream), ordered on `stream` (the
@@ -827,6 +888,21 @@ class BeamformerPipeline {
     }
 
   private:
+    Description describe_base(std::size_t dm_idx) const
+    {
+        if(dm_idx >= _config.coherent_dms().size())
+            throw std::runtime_error("BeamformerPipeline: DM index out of range");
+        int fft_len = 0, overlap = 0;
+        check(sw_pipeline_fft_len(_p, &fft_len, &overlap));
+        const double chan_tsamp = (double)_config.nchans() / _config.bandwidth();
+        Description d;
+        d.freqs         = _config.channel_frequencies();
+        d.sample_period = chan_tsamp;
+        d.offset        = chan_tsamp * overlap / 2.0;  // CoherentDedisperser.cu:82
+        d.coherent_dm   = _config.coherent_dms()[dm_idx];
+        return d;
+    }
+
     const PipelineConfig& _config;
     CBHandler& _cb;
     DelayManager _delays;

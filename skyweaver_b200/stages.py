@@ -324,6 +324,23 @@ class IncoherentDedispersionPipeline:
 
 
 # ------------------------------------------------------------------ pipeline
+def describe(dims, sizes, centre_frequency, bandwidth, nchans, tscrunch, overlap, dm):
+    """The metadata the reference's DescribedVector carries beside its data
+    (DescribedVector.hpp:96-573) for one pipeline output: dimension order and
+    extents, channel centre frequencies (PipelineConfig.cpp:188-203), tsamp =
+    tscrunch x channel sample (CoherentBeamformer.cu:235), utc_offset = the
+    coherent dedisperser's filter delay tsamp * overlap / 2
+    (CoherentDedisperser.cu:82) and reference_dm = the coherent DM
+    (CoherentDedisperser.cu:224)."""
+    chbw = bandwidth / nchans
+    bottom = centre_frequency - bandwidth / 2.0
+    chan_tsamp = nchans / bandwidth
+    return {"dims": dims, "extents": tuple(int(x) for x in sizes),
+            "frequencies": [bottom + chbw / 2.0 + chbw * i for i in range(nchans)],
+            "tsamp": chan_tsamp * tscrunch, "utc_offset": chan_tsamp * overlap / 2.0,
+            "dms": [], "reference_dm": float(dm)}
+
+
 class BeamformerPipeline:
     """sw_pipeline_*: the graph-captured per-gulp chain (BeamformerPipeline)."""
 
@@ -351,11 +368,32 @@ class BeamformerPipeline:
         self.nbeamsets = bw.shape[0]
         self._nant = nantennas
         self.stokes = stokes
+        self._centre, self._bandwidth = float(centre_frequency), float(bandwidth)
+        self._dm_list = [float(d) for d in dms]
+        self._ib_tscrunch = tscrunch
 
     def close(self):
         if self.h:
             lib().sw_pipeline_destroy(self.h)
             self.h = None
+
+    def _describe(self, dm_idx, dims, sizes, tscrunch):
+        if not 0 <= dm_idx < self.ndms:
+            raise IndexError(f"DM index {dm_idx} out of range")
+        _, overlap = self.fft_plan()
+        return describe(dims, sizes, self._centre, self._bandwidth, self.nchans, tscrunch,
+                        overlap, self._dm_list[dm_idx])
+
+    def describe_cb(self, dm_idx: int) -> dict:
+        """DescribedVector metadata of one DM's coherent beams (TFB): the
+        description the reference's CB handler finds on its TFBPowersD."""
+        return self._describe(dm_idx, "TFB", (self.gulp // self.tscrunch, self.nchans,
+                                              self.nbeams), self.tscrunch)
+
+    def describe_ib(self, dm_idx: int) -> dict:
+        """The same for the incoherent beams (BTF over beamsets)."""
+        return self._describe(dm_idx, "BTF", (self.nbeamsets, self.gulp // self._ib_tscrunch,
+                                              self.nchans), self._ib_tscrunch)
 
     def __del__(self):
         try:

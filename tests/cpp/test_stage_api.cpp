@@ -253,6 +253,20 @@ static void pipeline_smoke(const std::string& golden)
     for(int g = 0; g < 3; ++g) pipe(taftp.data(), 1708082168.957 + 1.0 + g * 0.02);
     EXPECT(h.calls == 6);
     EXPECT(h.bytes == 6 * (4096 / 16) * c.nchans() * c.nbeams());
+    // DescribedVector metadata of the outputs (CoherentBeamformer.cu:231-235)
+    const Description d = pipe.describe_cb(1);
+    EXPECT(d.dims_as_string() == "TFB");
+    EXPECT(d.extents() == std::vector<std::size_t>({4096 / 16, c.nchans(), c.nbeams()}));
+    EXPECT(d.nsamples() == 4096 / 16 && d.nchannels() == c.nchans() && d.nbeams() == c.nbeams());
+    EXPECT(d.frequencies() == c.channel_frequencies());
+    const double chan_tsamp = (double)c.nchans() / c.bandwidth();
+    EXPECT(std::fabs(d.tsamp() - 16 * chan_tsamp) < 1e-15);
+    EXPECT(d.reference_dm() == 5.0f && d.utc_offset() >= 0.0);
+    const Description ib = pipe.describe_ib(0);
+    EXPECT(ib.dims_as_string() == "BTF" && ib.nsamples() == 4096 / 16);
+    bool threw = false;
+    try { pipe.describe_cb(2); } catch(const std::runtime_error&) { threw = true; }
+    EXPECT(threw);
     std::puts("PASS beamformer_pipeline");
 }
 

@@ -140,3 +140,19 @@ def test_c_abi_rejects_bad_arguments_without_gpu():
     assert b"null" in L.sw_last_error()
     assert L.sw_cdd_setup_bytes(1, 1, 1000) == 0      # not a power of two
     assert L.sw_cdd_setup_bytes(2, 4, 4096) > 2 * 4 * 4096 * 8
+
+
+def test_output_description_follows_described_vector():
+    """stages.describe: the DescribedVector metadata of a pipeline output
+    (DescribedVector.hpp:96-573, CoherentBeamformer.cu:235,
+    CoherentDedisperser.cu:82,224, PipelineConfig.cpp:188-203)."""
+    from skyweaver_b200 import stages
+    d = stages.describe("TFB", (4096, 64, 1024), 1284e6, 64 * 856e6 / 1024, 64, 16, 1472, 150.0)
+    chbw = 856e6 / 1024
+    assert d["dims"] == "TFB" and d["extents"] == (4096, 64, 1024)
+    assert len(d["frequencies"]) == 64
+    assert abs(d["frequencies"][0] - (1284e6 - 32 * chbw + chbw / 2)) < 1e-3
+    assert abs(d["frequencies"][63] - (1284e6 + 32 * chbw - chbw / 2)) < 1e-3
+    assert abs(d["tsamp"] - 16 / chbw) < 1e-15
+    assert abs(d["utc_offset"] - 736 / chbw) < 1e-15
+    assert d["reference_dm"] == 150.0 and d["dms"] == []

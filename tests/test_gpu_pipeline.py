@@ -124,6 +124,12 @@ def test_ragged_beamsets_grouped_equals_plain_and_oracle(cuda, oracle):
         fft_len, overlap = pipe.fft_plan()
         pipe.process_device(torch.from_numpy(taftp).cuda(), 1.7e9)
         outs[name] = [pipe.outputs(d) for d in range(len(dms))]
+        # the DescribedVector metadata of the outputs
+        d = pipe.describe_cb(1)
+        assert d["dims"] == "TFB" and d["extents"] == (T // ts, F, B)
+        assert d["reference_dm"] == 50.0 and abs(d["tsamp"] - ts / chbw) < 1e-15
+        assert abs(d["utc_offset"] - overlap / 2 / chbw) < 1e-15
+        assert pipe.describe_ib(0)["extents"] == (len(beams), T // ts, F)
         pipe.close()
     for a, b in zip(outs["grouped"], outs["plain"]):
         assert np.array_equal(a["cb"], b["cb"])
