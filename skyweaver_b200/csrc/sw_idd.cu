@@ -10,8 +10,12 @@
 // by dp4a(word, 1 << 8b, acc), one instruction per addition on the integer
 // multiply-add pipe.  (Biasing each word to unsigned and adding pairs of
 // 16-bit lanes, two per instruction, measured 8 % slower: it needs a xor and
-// two byte permutes per word on the pipe that also issues the adds.)  The
-// final float divide is the reference's single IEEE division.
+// two byte permutes per word on the pipe that also issues the adds.  Half
+// the words through dp4a and half through that 16-bit path, to load both
+// integer pipes, measured the same as dp4a alone: 17.4-17.8 vs 17.8-17.9 ms
+// on the 128-DM UHF case, where L2 latency, not the multiply-add pipe alone,
+// sets the pace.)  The final float divide is the reference's single IEEE
+// division.
 #include "sw_common.cuh"
 
 namespace swb {

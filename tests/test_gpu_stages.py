@@ -408,6 +408,32 @@ def test_incoherent_dedispersion_exact(cuda, oracle):
     assert np.array_equal(_np(got), ref)
 
 
+@pytest.mark.parametrize("fill", ["random", -128, 127])
+def test_incoherent_dedispersion_many_channels(cuda, oracle, fill):
+    """More than 256 terms per sum (301 channels x tscrunch 3, an odd channel
+    count) at the int8 extremes: the 16-bit partial sums of the 16-beam path
+    are flushed every 256 channels, and every sum must still be exact."""
+    from skyweaver_b200 import stages, synthetic
+    g = synthetic.rng(43)
+    F, B, ts = 301, 48, 3
+    freqs = synthetic.channel_frequencies(1284e6, 64 * 856e6 / 1024, F)
+    dms = np.array([0, 3, 7], np.float32)
+    delays, maxd = oracle.idd_delays(freqs, dms, 16 / (856e6 / 1024))
+    T = maxd + 16 * ts
+    if fill == "random":
+        tfb = g.integers(-128, 128, size=(T, F, B), dtype=np.int8)
+        sf = np.float32(64.0)
+    else:
+        tfb = np.full((T, F, B), fill, np.int8)
+        sf = np.float32(1000.0)
+    ref = oracle.idd(tfb, delays, maxd, ts, sf)
+    got = _np(stages.incoherent_dedisperse(_dev(cuda, tfb), _dev(cuda, delays), maxd, ts,
+                                           float(sf)))
+    assert np.array_equal(got, ref)
+    if fill != "random":
+        assert np.all(ref == int(fill * F * ts / 1000.0))
+
+
 def test_incoherent_dedispersion_ones(cuda, oracle):
     """IncoherentDedisperserTester.cu:96-126: all-ones input -> sqrt(F*ts)."""
     from skyweaver_b200 import stages, synthetic
