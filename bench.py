@@ -656,7 +656,8 @@ def profile_case(which, nchans=16, reps=3):
     benchmark workload (268 MB of voltages for 16 channels, above L2), one
     warm-up launch and `reps` profiled launches of one kernel.  `idd`: the
     UHF incoherent-dedispersion trials (128 DMs over 0-100, 256 channels,
-    2048 beams) on 4096 output samples, a 5.9 GB beam buffer."""
+    2048 beams) on 4096 output samples, a 5.9 GB beam buffer.  `bw`: the
+    transpose, statistics and incoherent-beam kernels on the same channels.""" 
     import torch
 
     from skyweaver_b200 import stages, synthetic
@@ -683,6 +684,24 @@ def profile_case(which, nchans=16, reps=3):
     F = nchans
     dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
     gen = torch.Generator(device="cuda").manual_seed(7)
+    if which == "bw":
+        # the HBM-bound stages of one gulp: TAFTP -> FPACT transpose, statistics,
+        # and the incoherent beam of one DM
+        # complex-Gaussian sigma = 8 voltages, as in the workload (full-range
+        # uniform bytes would push the incoherent beam's integer sums past 2^24
+        # and onto its reference-order float path)
+        taftp = (torch.randn((T // 256, A, F, 256, 2, 2), generator=gen, device="cuda") * 8)
+        taftp = taftp.round_().clamp_(-127, 127).to(torch.int8)
+        fpact = stages.transpose_fpact(taftp, A)
+        bw = dev(np.ones((1, A), np.float32))
+        scl = dev(np.full(F, 1e4, np.float32))
+        for _ in range(1 + reps):
+            stages.transpose_fpact(taftp, A, out=fpact)
+            stages.statistics(fpact, T)
+            stages.incoherent_beamform(fpact, T, ts, scl, scl, bw)
+        torch.cuda.synchronize()
+        print(f"profile case bw: {nchans} channels, {1 + reps} launches of each stage ok")
+        return
     fp = (torch.randn((F, 2, A, 2, T), generator=gen, device="cuda") * 8).round_().clamp_(-127, 127)
     fp = fp.to(torch.int8)
     if which == "cb":
@@ -712,7 +731,7 @@ def profile_case(which, nchans=16, reps=3):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--profile", choices=["cb", "cdd", "idd"], default=None,
+    ap.add_argument("--profile", choices=["cb", "cdd", "idd", "bw"], default=None,
                     help="run a small single-kernel case for ncu and exit")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
