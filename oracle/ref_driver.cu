@@ -12,8 +12,8 @@
 // (src/IncoherentBeamformer.cu:108-182, src/CoherentBeamformer.cu:191-270),
 // WeightsManager::weights (src/WeightsManager.cu:109-139),
 // IncoherentDedisperser::dedisperse (src/IncoherentDedisperser.cu:66-125) and
-// CoherentDedisperser::dedisperse (src/CoherentDedisperser.cu:142-225, timed
-// only).
+// CoherentDedisperser::dedisperse (src/CoherentDedisperser.cu:142-225, one
+// window, and timed over a gulp).
 #include <cstring>
 #include <stdexcept>
 #include <vector>
@@ -216,6 +216,33 @@ int swref_time_cdd(int fft_length, int overlap, const float* dms, int ndms, doub
         *ms /= reps;
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
+    });
+}
+
+// One overlap-save window of one channel through the reference's
+// CoherentDedisperser::dedisperse (src/CoherentDedisperser.cu:142-225, cuFFT
+// in FP32): TPA char2 [fft_length][2][NANT] of channel `chan` in, the trimmed
+// [fft_length - overlap][2][NANT] char2 of that channel and DM out.  The
+// band is [low, low + bw) over the build's SKYWEAVER_NCHANS channels.
+int swref_cdd(int fft_length, int overlap, const float* dms, int ndms, double low, double bw,
+              int chan, int dm_idx, const int8_t* tpa, int8_t* out_tpa)
+{
+    return guarded([&] {
+        PipelineConfig& c = config(low + bw / 2, bw);
+        CoherentDedisperserConfig cfg;
+        create_coherent_dedisperser_config(cfg, fft_length, overlap, c.nchans(), c.npol(),
+                                           c.nantennas(), c.nchans() / bw, low, bw,
+                                           std::vector<float>(dms, dms + ndms));
+        CoherentDedisperser cd(cfg);
+        TPAVoltagesH<char2> h({(std::size_t)fft_length, c.npol(), c.nantennas()});
+        std::memcpy(thrust::raw_pointer_cast(h.data()), tpa, h.size() * 2);
+        TPAVoltagesD<char2> in = h;
+        FTPAVoltagesD<char2> out({c.nchans(), (std::size_t)(fft_length - overlap), c.npol(),
+                                  c.nantennas()});
+        cd.dedisperse(in, out, chan, dm_idx);
+        thrust::host_vector<char2> back = out.vector();
+        const std::size_t per = (std::size_t)(fft_length - overlap) * c.npol() * c.nantennas();
+        std::memcpy(out_tpa, thrust::raw_pointer_cast(back.data()) + chan * per, per * 2);
     });
 }
 

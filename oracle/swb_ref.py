@@ -102,6 +102,23 @@ def idd(tfb, dms, tscrunch, centre, bw):
     return out[:n * len(dms) * s["nbeams"]].reshape(n, len(dms), s["nbeams"]), delays, maxd.value
 
 
+def cdd(tpa, overlap, dms, dm_idx, chan, low, bw):
+    """One overlap-save window of channel `chan` through the reference's
+    CoherentDedisperser (cuFFT): int8 TPA [fft_length][2][A][2] in, the
+    trimmed [fft_length - overlap][2][A][2] int8 for DM `dm_idx` out.  The
+    band [low, low + bw) spans the build's channels."""
+    tpa = np.ascontiguousarray(tpa, np.int8)
+    n = tpa.shape[0]
+    dms = np.ascontiguousarray(dms, np.float32)
+    out = np.empty((n - overlap,) + tpa.shape[1:], np.int8)
+    lib().swref_cdd.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                ctypes.c_void_p, ctypes.c_void_p]
+    _check(lib().swref_cdd(n, overlap, _p(dms), len(dms), low, bw, chan, dm_idx, _p(tpa),
+                           _p(out)))
+    return out
+
+
 LIB_C1 = os.path.join(HERE, "_ref", "c1", "libswref_c1.so")
 
 
