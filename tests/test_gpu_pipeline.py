@@ -88,6 +88,7 @@ def test_pipeline_matches_oracle_chain(cuda, oracle, use_graph, grouped):
             assert np.array_equal(out["cb"], cb_ref)
         else:
             diff = np.abs(out["cb"].astype(int) - cb_ref.astype(int))
+            print(f"pipeline DM {dm}: {(diff > 0).sum()} of {diff.size} beams differ")
             assert (diff > 0).mean() < 2e-3, (diff > 0).mean()
             assert np.allclose(out["ib_raw"], raw_ref, rtol=1e-3)
 

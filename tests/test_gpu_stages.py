@@ -320,8 +320,9 @@ def test_coherent_dedispersion_golden_vector(cuda):
     outs = cdd.dedisperse(fp, 1024 - overlap)
     got = _np(outs[1])[0].transpose(3, 0, 1, 2)                # [446][P][A][C]
     diff = np.abs(got.astype(int) - want.astype(int))
+    print(f"golden DM 1000: {(diff > 0).sum()} of {diff.size} differ by one LSB")
     assert diff.max() <= 1                                     # reference tolerance
-    assert (diff > 0).mean() < 1e-3
+    assert (diff > 0).mean() <= 1e-5                           # measured: 1 of 114176
     # DM 0 is the identity shifted by overlap/2 (CoherentDedisperserTester.cu:69-111)
     got0 = _np(outs[0])[0].transpose(3, 0, 1, 2)
     assert np.abs(got0.astype(int) - inp[overlap // 2: overlap // 2 + 446].astype(int)).max() <= 1
@@ -351,8 +352,9 @@ def test_coherent_dedispersion_overlap_save(cuda, oracle, fft_len, dms):
         got = _np(outs[d]).transpose(0, 4, 1, 2, 3)
         diff = np.abs(got.astype(int) - ref.astype(int))
         frac = (diff > 0).mean()
+        print(f"fft {fft_len} DM {dm}: {(diff > 0).sum()} of {diff.size} differ by one LSB")
         assert diff.max() <= 1, (dm, diff.max())
-        assert frac < 1e-3, (dm, frac)
+        assert frac <= 1e-5, (dm, frac)                       # measured: at most 2 of 262144
 
 
 def test_coherent_dedispersion_fft65536_precision(cuda, oracle):
@@ -388,7 +390,8 @@ def test_coherent_dedispersion_fft65536_precision(cuda, oracle):
         assert err.max() < 0.05, (dm, err.max())
         got = _np(outs[d]).transpose(0, 4, 1, 2, 3)
         diff = np.abs(got.astype(int) - ref.astype(int))
-        assert diff.max() <= 1 and (diff > 0).mean() < 1e-3, (dm, (diff > 0).mean())
+        print(f"fft 65536 DM {dm}: {(diff > 0).sum()} of {diff.size} differ by one LSB")
+        assert diff.max() <= 1 and (diff > 0).mean() <= 1e-5, (dm, (diff > 0).mean())
 
 
 # ------------------------------------------------- incoherent dedispersion
