@@ -50,6 +50,39 @@ def tsamp():
     return 1.0 / WORK["chbw"]
 
 
+RFI_CHANNELS = (9, 27, 45)
+PULSE_EVERY = 20  # one gulp in 20 carries the DM-100 pulse (the step index = 10 mod 20)
+INPUTS = ("complex Gaussian sigma 8 int8 voltages; narrowband RFI tones at 20 sigma in "
+          "channels 9, 27 and 45; a DM-100 pulse (64 samples, +3 sigma) in every 20th gulp")
+
+
+def workload_gulp(torch, gen, centre, bwidth, pulse):
+    """One gulp of the benchmark workload on the device, TAFTP int8: complex
+    Gaussian voltages (sigma 8 per component), three narrowband RFI tones at
+    20 sigma and, when `pulse`, a DM-100 burst dispersed across the subband
+    (arrival at the top channel a quarter into the gulp)."""
+    from skyweaver_b200 import synthetic
+    A, F, T = WORK["nant"], WORK["nchans"], WORK["gulp"]
+    v = torch.randn((T // 256, A, F, 256, 2, 2), generator=gen, device="cuda") * 8.0
+    t = torch.arange(T, device="cuda", dtype=torch.float32).reshape(T // 256, 256)
+    for k, c in enumerate(RFI_CHANNELS):
+        ph = 2 * math.pi * (0.01 + 0.037 * k) * t
+        tone = torch.stack([160.0 * torch.cos(ph), 160.0 * torch.sin(ph)], -1)  # [h][s][2]
+        v[:, :, c] += tone[:, None, :, None, :]
+    if pulse:
+        freqs = synthetic.channel_frequencies(centre, bwidth, F)
+        fref = freqs.max()
+        for c, f in enumerate(freqs):
+            s0 = T // 4 + int(round(synthetic.DM_CONST * 100.0 * (1 / f ** 2 - 1 / fref ** 2)
+                                    / tsamp()))
+            idx = torch.arange(s0, min(T, s0 + 64), device="cuda")
+            if idx.numel():
+                h, smp = idx // 256, idx % 256
+                v[h, :, c, smp] += torch.randn((idx.numel(), A, 2, 2), generator=gen,
+                                               device="cuda") * 24.0
+    return v.round_().clamp_(-127, 127).to(torch.int8)
+
+
 def config_block(extra=None):
     c = {"workload": "64ant x 1024beam x 64ch x 65536-sample gulps, 4 coherent DMs "
                      "{0,50,150,500}, Stokes I, tscrunch 16 (L-band 1284 MHz subband)",
@@ -282,9 +315,9 @@ def main_b200(args):
     g = synthetic.rng(1000 + rank)
     delays = synthetic.delay_model(g, B, A)
     gen = torch.Generator(device="cuda").manual_seed(1234 + rank)
-    nheaps = T // 256
-    taftp = (torch.randn((nheaps, A, F, 256, 2, 2), generator=gen, device="cuda") * 8.0)
-    taftp = taftp.round_().clamp_(-127, 127).to(torch.int8)
+    taftp = workload_gulp(torch, gen, centre, bwidth, pulse=False)
+    taftp_pulse = workload_gulp(torch, gen, centre, bwidth, pulse=True)
+    gulp = lambda i: taftp_pulse if i % PULSE_EVERY == 10 else taftp
     bwts = np.ones((1, A), np.float32)
     mapping = np.zeros(B, np.int32)
     common = dict(nantennas=A, input_nantennas=A, nchans=F, nbeams=B, gulp_samples=T,
@@ -316,7 +349,7 @@ def main_b200(args):
 
     # ---- headline: batched grouped CB + CUDA graph, input resident in HBM
     with Clocks(local) as clk:
-        ms_graph = time_steps(lambda i: pipe.process_device(taftp, epoch0 + i * gulp_s),
+        ms_graph = time_steps(lambda i: pipe.process_device(gulp(i), epoch0 + i * gulp_s),
                               args.steps, args.warmup)
     clocks = clk.summary()
     rtf = gulp_s / (ms_graph * 1e-3)
@@ -325,7 +358,7 @@ def main_b200(args):
     # ---- plain GPU form: one CB launch per (DM, beamset), no graph
     plain = stages.BeamformerPipeline(**common, grouped=False, use_graph=False)
     plain.set_delays(delays, 1.7e9)
-    ms_plain = time_steps(lambda i: plain.process_device(taftp, epoch0 + i * gulp_s),
+    ms_plain = time_steps(lambda i: plain.process_device(gulp(i), epoch0 + i * gulp_s),
                           max(3, args.steps // 2), 2)
     plain.close()
     del plain
@@ -341,11 +374,15 @@ def main_b200(args):
     long_fft = long_fft_case(torch, stages, synthetic, taftp, common, args.steps)
 
     # ---- end to end through the host API (pinned H2D + D2H inside the timing)
-    h_in = torch.empty(taftp.shape, dtype=torch.int8, pin_memory=True)
-    h_in.copy_(taftp)
+    h_ins = []
+    for g_dev in (taftp, taftp_pulse):
+        h_ins.append(torch.empty(taftp.shape, dtype=torch.int8, pin_memory=True))
+        h_ins[-1].copy_(g_dev)
+    h_in = h_ins[0]
     cb_bytes = pipe.cb_bytes_per_dm() * len(dms)
     h_out = torch.empty(cb_bytes, dtype=torch.int8, pin_memory=True)
-    ms_e2e = time_steps(lambda i: pipe.process_host(h_in, epoch0 + i * gulp_s, h_out),
+    ms_e2e = time_steps(lambda i: pipe.process_host(h_ins[i % PULSE_EVERY == 10],
+                                                    epoch0 + i * gulp_s, h_out),
                         args.steps, args.warmup)
     e2e = {"value": gulp_s / (ms_e2e * 1e-3) * world, "unit": "x real-time",
            "h2d_bytes_per_step": int(h_in.numel()), "d2h_bytes_per_step": int(cb_bytes),
@@ -377,7 +414,7 @@ def main_b200(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_graph,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int8",
             "data": "synthetic", "impl": "b200",
-            "config": config_block({"fft_len": fft_len, "overlap": overlap,
+            "config": config_block({"fft_len": fft_len, "overlap": overlap, "inputs": INPUTS,
                                     "parallelism": f"{world} independent subbands"}),
             "int8_tops_pipeline": ops_gulp / (ms_graph * 1e-3) / 1e12,
             "cb_int8_tops": cb["tops"],
