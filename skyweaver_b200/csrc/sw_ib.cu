@@ -22,6 +22,14 @@ namespace {
 
 constexpr int kMaxBs = 8;          // beamsets per pass (registers)
 constexpr int kMaxAnt = 256;
+constexpr int kTableAnt = 64;  // antennas of the float-chain product table (4 KB a thread)
+
+// signed byte k (0..15, unrolled) of a 16-byte load
+__device__ __forceinline__ int sbyte(const uint4& v, int k)
+{
+    const uint32_t w = k < 4 ? v.x : k < 8 ? v.y : k < 12 ? v.z : v.w;
+    return (int)(int8_t)(w >> (8 * (k & 3)));
+}
 
 struct IbArgs {
     const uint8_t* fpact;
@@ -162,6 +170,36 @@ ib_k(IbArgs args, int bs0)
             float power;
             if(s_intw[s] && B[s] <= (1ll << 24)) {
                 power = (float)S[s * NC + c];  // the float chain is exact
+            } else if(quads && args.nant <= kTableAnt) {
+                // reference order (t outer, a inner) from a table of the
+                // products: each antenna's four 16-sample rows are read once
+                // with 16-byte loads, the 16 x nant products go to a
+                // per-thread table in local memory (lane-interleaved, so
+                // coalesced and mostly L1/L2 resident), and the chain then
+                // walks the table.  Walking the rows byte by byte in chain
+                // order instead re-reads every row once per sample, because
+                // the warp's 4 rows x nant windows do not stay in L1.
+                power = 0.0f;
+                for(int tc = 0; tc < args.tscrunch; tc += 16) {
+                    float x[16][kTableAnt];
+#pragma unroll 4
+                    for(int a = 0; a < args.nant; ++a) {
+                        const uint8_t* q0 = args.fpact + (((size_t)f * P + 0) * args.nant + a) * 2 * args.row_stride + args.offset + t0 + tc;
+                        const uint8_t* q1 = args.fpact + (((size_t)f * P + 1) * args.nant + a) * 2 * args.row_stride + args.offset + t0 + tc;
+                        const uint4 R0 = *reinterpret_cast<const uint4*>(q0);
+                        const uint4 I0 = *reinterpret_cast<const uint4*>(q0 + args.row_stride);
+                        const uint4 R1 = *reinterpret_cast<const uint4*>(q1);
+                        const uint4 I1 = *reinterpret_cast<const uint4*>(q1 + args.row_stride);
+                        const float w = sw[s][a];
+#pragma unroll
+                        for(int k = 0; k < 16; ++k)
+                            x[k][a] = fmul(stokes_f(stokes, (float)sbyte(R0, k), (float)sbyte(I0, k),
+                                                    (float)sbyte(R1, k), (float)sbyte(I1, k)),
+                                           w);
+                    }
+                    for(int k = 0; k < 16; ++k)
+                        for(int a = 0; a < args.nant; ++a) power = fadd(power, x[k][a]);
+                }
             } else {
                 // reference order: t outer, a inner, float multiply and add
                 power = 0.0f;
