@@ -56,15 +56,15 @@ INPUTS = ("complex Gaussian sigma 8 int8 voltages; narrowband RFI tones at 20 si
           "channels 9, 27 and 45; a DM-100 pulse (64 samples, +3 sigma) in every 20th gulp")
 
 
-def workload_gulp(torch, gen, centre, bwidth, pulse):
+def workload_gulp(torch, gen, centre, bwidth, pulse, device="cuda"):
     """One gulp of the benchmark workload on the device, TAFTP int8: complex
     Gaussian voltages (sigma 8 per component), three narrowband RFI tones at
     20 sigma and, when `pulse`, a DM-100 burst dispersed across the subband
     (arrival at the top channel a quarter into the gulp)."""
     from skyweaver_b200 import synthetic
     A, F, T = WORK["nant"], WORK["nchans"], WORK["gulp"]
-    v = torch.randn((T // 256, A, F, 256, 2, 2), generator=gen, device="cuda") * 8.0
-    t = torch.arange(T, device="cuda", dtype=torch.float32).reshape(T // 256, 256)
+    v = torch.randn((T // 256, A, F, 256, 2, 2), generator=gen, device=device) * 8.0
+    t = torch.arange(T, device=device, dtype=torch.float32).reshape(T // 256, 256)
     for k, c in enumerate(RFI_CHANNELS):
         ph = 2 * math.pi * (0.01 + 0.037 * k) * t
         tone = torch.stack([160.0 * torch.cos(ph), 160.0 * torch.sin(ph)], -1)  # [h][s][2]
@@ -75,11 +75,11 @@ def workload_gulp(torch, gen, centre, bwidth, pulse):
         for c, f in enumerate(freqs):
             s0 = T // 4 + int(round(synthetic.DM_CONST * 100.0 * (1 / f ** 2 - 1 / fref ** 2)
                                     / tsamp()))
-            idx = torch.arange(s0, min(T, s0 + 64), device="cuda")
+            idx = torch.arange(s0, min(T, s0 + 64), device=device)
             if idx.numel():
                 h, smp = idx // 256, idx % 256
                 v[h, :, c, smp] += torch.randn((idx.numel(), A, 2, 2), generator=gen,
-                                               device="cuda") * 24.0
+                                               device=device) * 24.0
     return v.round_().clamp_(-127, 127).to(torch.int8)
 
 

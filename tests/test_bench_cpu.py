@@ -39,3 +39,26 @@ def test_clock_summary_reads_nvidia_smi_rows(tmp_path):
     s = c.summary()
     assert s["samples"] == 2 and s["reasons"] == ["sw_power_cap"]
     assert s["source"] == "nvidia-smi 200 ms"
+
+
+def test_workload_gulp_tones_and_pulse(monkeypatch):
+    """The benchmark gulp (here 2 antennas): sigma-8 voltages, the three RFI
+    channels saturated by their tones, and the DM-100 pulse a quarter into the
+    gulp at the top channel, arriving later in lower channels."""
+    import torch
+    monkeypatch.setitem(bench.WORK, "nant", 2)
+    centre, bw = bench.WORK["centre"], bench.WORK["nchans"] * bench.WORK["chbw"]
+    gen = torch.Generator().manual_seed(1)
+    v = bench.workload_gulp(torch, gen, centre, bw, pulse=True, device="cpu")
+    T, F = bench.WORK["gulp"], bench.WORK["nchans"]
+    assert v.shape == (T // 256, 2, F, 256, 2, 2) and v.dtype == torch.int8
+    level = v.float().abs().mean(dim=(0, 1, 3, 4, 5))           # per channel
+    quiet = [c for c in range(F) if c not in bench.RFI_CHANNELS]
+    assert level[quiet].max() < 8 and level[list(bench.RFI_CHANNELS)].min() > 80
+    power = (v.float() ** 2).sum(dim=(1, 4, 5)).permute(1, 0, 2).reshape(F, T)
+    peak = power.argmax(dim=1)
+    assert abs(int(peak[F - 1]) - T // 4) < 64
+    assert int(peak[0]) > int(peak[F // 2]) > int(peak[F - 1])
+    plain = bench.workload_gulp(torch, gen, centre, bw, pulse=False, device="cpu")
+    assert (plain.float() ** 2).sum(dim=(1, 4, 5)).permute(1, 0, 2).reshape(F, T)[0].max() < \
+        power[0].max()
