@@ -26,6 +26,14 @@ namespace swb {
 int launch_weights(const float* d_delays, const double* d_freqs, int nant, int nbeams,
                    int nchans, double current_epoch, double delay_epoch,
                    const double* d_epochs, void* d_fba, void* d_gemm, cudaStream_t stream);
+int launch_incoherent_beamform(const void* d_fpact, size_t row_stride, size_t sample_offset,
+                               int nchans, int nsamples, int nant, int tscrunch,
+                               const float* d_scale, const float* d_offset,
+                               const float* d_beamset_weights, int nbeamsets, int stokes,
+                               float* d_raw, int8_t* d_out, cudaStream_t stream,
+                               const int* d_chan_order);
+int launch_ib_channel_order(const float* d_stats, int nchans, int npol, int nant,
+                            int* d_order, cudaStream_t stream);
 }
 
 namespace {
@@ -71,6 +79,7 @@ struct sw_pipeline {
     DevBuf ext;
     std::vector<DevBuf> dd;
     DevBuf stats, stats_scratch;
+    DevBuf ib_order;  // channels by descending power, for the incoherent beam
     DevBuf cb_off, cb_scl, ib_off, ib_scl;
     DevBuf d_bw, d_map, d_delays, d_freqs, d_wgemm, d_setup, cdd_ws;
     DevBuf epochs;  // [2 parities][2] doubles
@@ -195,6 +204,7 @@ int sw_pipeline::init(const sw_pipeline_config& c)
     }
     SW_TRY(stats.alloc((size_t)F * 2 * A * 4 * sizeof(float)));
     SW_TRY(stats_scratch.alloc(sw_statistics_scratch_bytes(F, 2, A)));
+    if(F <= swb::kIbOrderMaxChans) SW_TRY(ib_order.alloc((size_t)F * sizeof(int)));
     for(DevBuf* b : {&cb_off, &cb_scl, &ib_off, &ib_scl}) SW_TRY(b->alloc((size_t)S * F * sizeof(float)));
     SW_TRY(d_bw.alloc(bw.size() * sizeof(float)));
     SW_TRY(d_map.alloc(mapping.size() * sizeof(int)));
@@ -234,6 +244,11 @@ int sw_pipeline::enqueue_chain(const void* d_in, int parity, bool first)
                               ext_off, ss));
     SW_TRY(sw_statistics(ext.p, ext_stride, ext_off, F, 2, A, T, stats_scratch.p,
                          stats.as<float>(), ss));
+    const int* chan_order = nullptr;
+    if(ib_order.p) {
+        SW_TRY(swb::launch_ib_channel_order(stats.as<float>(), F, 2, A, ib_order.as<int>(), s));
+        chan_order = ib_order.as<int>();
+    }
     if(first) {
         SW_TRY(sw_update_scalings(stats.as<float>(), d_bw.as<float>(), S, F, 2, A, ts, ts,
                                   cfg.output_level, cb_off.as<float>(), cb_scl.as<float>(),
@@ -255,10 +270,11 @@ int sw_pipeline::enqueue_chain(const void* d_in, int parity, bool first)
         for(int d = 0; d < ndm; ++d) volt[d] = ext.p;
     }
     for(int d = 0; d < ndm; ++d) {
-        SW_TRY(sw_incoherent_beamform(volt[d], vstride, voff, F, T, A, ts, ib_scl.as<float>(),
-                                      ib_off.as<float>(), d_bw.as<float>(), S, cfg.stokes,
-                                      ib_raw[parity][d].as<float>(),
-                                      ib_i8[parity][d].as<int8_t>(), ss));
+        SW_TRY(swb::launch_incoherent_beamform(volt[d], vstride, voff, F, T, A, ts,
+                                               ib_scl.as<float>(), ib_off.as<float>(),
+                                               d_bw.as<float>(), S, cfg.stokes,
+                                               ib_raw[parity][d].as<float>(),
+                                               ib_i8[parity][d].as<int8_t>(), s, chan_order));
     }
     sw_cb_shape shape{F, T, A, B, ts, cfg.stokes, cfg.ib_subtract, vstride, voff, cb_tpi};
     if(cfg.grouped) {

@@ -59,6 +59,10 @@ inline cudaStream_t as_cuda(sw_stream_t s) { return reinterpret_cast<cudaStream_
 
 namespace swb {
 
+// Largest channel count for which the incoherent beam's channel order is
+// computed (one CTA ranks all channels in shared memory).
+constexpr int kIbOrderMaxChans = 1024;
+
 // ceil division
 template <typename T>
 __host__ __device__ constexpr T cdiv(T a, T b) { return (a + b - 1) / b; }

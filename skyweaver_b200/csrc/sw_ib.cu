@@ -38,6 +38,7 @@ struct IbArgs {
     const float *scale, *offset_v, *weights;
     float* raw;
     int8_t* out;
+    const int* chan_order;  // CTA row -> channel (nullptr: identity)
 };
 
 __device__ __forceinline__ float stokes_f(int stokes, float r0, float i0,
@@ -80,7 +81,7 @@ ib_k(IbArgs args, int bs0)
 
     const int nout = args.nsamples / args.tscrunch;
     const int tp = blockIdx.x * blockDim.x + threadIdx.x;
-    const int f  = blockIdx.y;
+    const int f  = args.chan_order ? args.chan_order[blockIdx.y] : (int)blockIdx.y;
     if(tp >= nout) return;
     const int t0 = tp * args.tscrunch;
     const size_t P = 2;
@@ -231,7 +232,7 @@ int launch_incoherent_beamform(const void* d_fpact, size_t row_stride,
                                const float* d_offset,
                                const float* d_beamset_weights, int nbeamsets,
                                int stokes, float* d_raw, int8_t* d_out,
-                               cudaStream_t stream)
+                               cudaStream_t stream, const int* d_chan_order)
 {
     SW_REQUIRE(d_fpact && d_scale && d_offset && d_beamset_weights && d_raw && d_out,
                "sw_incoherent_beamform: null pointer");
@@ -245,7 +246,7 @@ int launch_incoherent_beamform(const void* d_fpact, size_t row_stride,
     SW_REQUIRE(nchans > 0 && nchans <= 65535, "sw_incoherent_beamform: bad channel count");
     IbArgs args{static_cast<const uint8_t*>(d_fpact), row_stride, sample_offset,
                 nchans, nsamples, nant, tscrunch, nbeamsets, stokes, d_scale,
-                d_offset, d_beamset_weights, d_raw, d_out};
+                d_offset, d_beamset_weights, d_raw, d_out, d_chan_order};
     const int nout = nsamples / tscrunch;
     dim3 grid(cdiv(nout, 128), nchans);
     if(stokes == 4) {
@@ -262,6 +263,47 @@ int launch_incoherent_beamform(const void* d_fpact, size_t row_stride,
     return SW_OK;
 }
 
+namespace {
+
+// Channels in descending order of voltage power (sum over pols and antennas
+// of mean^2 + std^2, from the statistics stage).  The incoherent beam maps
+// its CTA rows through this order, so the channels most likely to need the
+// float chain (RFI-saturated ones, whose CTAs take longest) start first and
+// overlap the others instead of trailing behind them.  Ties go by channel
+// index and a NaN power counts as lowest, so the order is a permutation.
+__global__ void ib_channel_order_k(const float4* __restrict__ stats, int nchans, int npa,
+                                   int* __restrict__ order)
+{
+    extern __shared__ float pw[];
+    for(int c = threadIdx.x; c < nchans; c += blockDim.x) {
+        float s = 0.0f;
+        for(int i = 0; i < npa; ++i) {
+            const float4 v = stats[(size_t)c * npa + i];
+            s += v.x * v.x + v.y * v.y;
+        }
+        pw[c] = isnan(s) ? -1.0f : s;
+    }
+    __syncthreads();
+    for(int c = threadIdx.x; c < nchans; c += blockDim.x) {
+        int r = 0;
+        for(int k = 0; k < nchans; ++k) r += (pw[k] > pw[c]) || (pw[k] == pw[c] && k < c);
+        order[r] = c;
+    }
+}
+
+}  // namespace
+
+int launch_ib_channel_order(const float* d_stats, int nchans, int npol, int nant,
+                            int* d_order, cudaStream_t stream)
+{
+    SW_REQUIRE(d_stats && d_order, "ib channel order: null pointer");
+    SW_REQUIRE(nchans > 0 && nchans <= kIbOrderMaxChans, "ib channel order: bad channel count");
+    ib_channel_order_k<<<1, 256, nchans * sizeof(float), stream>>>(
+        reinterpret_cast<const float4*>(d_stats), nchans, npol * nant, d_order);
+    SW_LAUNCH_CHECK();
+    return SW_OK;
+}
+
 }  // namespace swb
 
 extern "C" int sw_incoherent_beamform(const void* d_fpact, size_t row_stride,
@@ -275,5 +317,5 @@ extern "C" int sw_incoherent_beamform(const void* d_fpact, size_t row_stride,
     return swb::launch_incoherent_beamform(
         d_fpact, row_stride, sample_offset, nchans, nsamples, nant, tscrunch,
         d_scale, d_offset, d_beamset_weights, nbeamsets, stokes, d_raw, d_out,
-        swb::as_cuda(stream));
+        swb::as_cuda(stream), nullptr);
 }

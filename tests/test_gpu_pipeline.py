@@ -16,7 +16,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def _run(cuda, oracle, use_graph, grouped):
+def _run(cuda, oracle, use_graph, grouped, tones=False):
     torch = cuda
     from skyweaver_b200 import stages, synthetic
     g = synthetic.rng(77)
@@ -47,6 +47,8 @@ def _run(cuda, oracle, use_graph, grouped):
     results = []
     for gulp in range(3):
         taftp = synthetic.voltages_taftp(g, T // 256, A_in, F, sigma=10)
+        if tones:  # saturated channels: the incoherent beam takes them first
+            synthetic.inject_tones(taftp, [1, 3], amplitude=160.0)
         epoch = epoch0 + gulp * T / chbw
         pipe.process_device(torch.from_numpy(taftp).cuda(), epoch)
         ftpa = oracle.transpose(taftp, A)
@@ -79,9 +81,10 @@ def pipe_stats(pipe, F, A):
     return _device_view(ptrs[3].value, n * 4).cpu().numpy().view(np.float32).reshape(F, 2, A, 4)
 
 
-@pytest.mark.parametrize("use_graph,grouped", [(True, True), (False, False)])
-def test_pipeline_matches_oracle_chain(cuda, oracle, use_graph, grouped):
-    for dm, out, raw_ref, ib_ref, cb_ref in _run(cuda, oracle, use_graph, grouped):
+@pytest.mark.parametrize("use_graph,grouped,tones",
+                         [(True, True, False), (False, False, False), (True, True, True)])
+def test_pipeline_matches_oracle_chain(cuda, oracle, use_graph, grouped, tones):
+    for dm, out, raw_ref, ib_ref, cb_ref in _run(cuda, oracle, use_graph, grouped, tones):
         if dm == 0.0:
             assert np.array_equal(out["ib_raw"], raw_ref)
             assert np.array_equal(out["ib"], ib_ref)
