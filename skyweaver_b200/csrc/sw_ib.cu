@@ -276,13 +276,16 @@ __global__ void ib_channel_order_k(const float4* __restrict__ stats, int nchans,
                                    int* __restrict__ order)
 {
     extern __shared__ float pw[];
-    for(int c = threadIdx.x; c < nchans; c += blockDim.x) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    for(int c = warp; c < nchans; c += nwarps) {  // one warp per channel
         float s = 0.0f;
-        for(int i = 0; i < npa; ++i) {
+        for(int i = lane; i < npa; i += 32) {
             const float4 v = stats[(size_t)c * npa + i];
             s += v.x * v.x + v.y * v.y;
         }
-        pw[c] = isnan(s) ? -1.0f : s;
+#pragma unroll
+        for(int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if(lane == 0) pw[c] = isnan(s) ? -1.0f : s;
     }
     __syncthreads();
     for(int c = threadIdx.x; c < nchans; c += blockDim.x) {
