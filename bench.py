@@ -164,7 +164,8 @@ def run_reference(args):
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int8", "data": "synthetic",
-            "config": config_block(),
+            "config": config_block({"inputs": INPUTS + " (the timed CPU sample is a Gaussian "
+                                    "slice: the CPU path's cost does not depend on the values)"}),
             "cpu_baseline": {k: vals[-1][k] for k in ("kind", "cores", "sample")} | {"value": v,
                                                                                    "unit": "x real-time"},
             "e2e": {"value": v, "unit": "x real-time", "h2d_bytes_per_step": 0,
