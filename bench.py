@@ -51,9 +51,23 @@ def tsamp():
 
 
 RFI_CHANNELS = (9, 27, 45)
+UHF_RFI_CHANNELS = (40, 130, 200)
 PULSE_EVERY = 20  # one gulp in 20 carries the DM-100 pulse (the step index = 10 mod 20)
 INPUTS = ("complex Gaussian sigma 8 int8 voltages; narrowband RFI tones at 20 sigma in "
           "channels 9, 27 and 45; a DM-100 pulse (64 samples, +3 sigma) in every 20th gulp")
+
+
+def add_rfi_tones(torch, v, channels):
+    """Narrowband RFI: a complex sinusoid of amplitude 160 per component (20
+    sigma of the sigma-8 voltages, clipped by the int8 conversion) added to
+    every antenna and pol of the given channels of a float TAFTP tensor
+    [heap][antenna][channel][256][pol][re, im]."""
+    t = torch.arange(v.shape[0] * 256, device=v.device, dtype=torch.float32)
+    t = t.reshape(v.shape[0], 256)
+    for k, c in enumerate(channels):
+        ph = 2 * math.pi * (0.01 + 0.037 * k) * t
+        tone = torch.stack([160.0 * torch.cos(ph), 160.0 * torch.sin(ph)], -1)  # [h][s][2]
+        v[:, :, c] += tone[:, None, :, None, :]
 
 
 def workload_gulp(torch, gen, centre, bwidth, pulse, device="cuda"):
@@ -64,11 +78,7 @@ def workload_gulp(torch, gen, centre, bwidth, pulse, device="cuda"):
     from skyweaver_b200 import synthetic
     A, F, T = WORK["nant"], WORK["nchans"], WORK["gulp"]
     v = torch.randn((T // 256, A, F, 256, 2, 2), generator=gen, device=device) * 8.0
-    t = torch.arange(T, device=device, dtype=torch.float32).reshape(T // 256, 256)
-    for k, c in enumerate(RFI_CHANNELS):
-        ph = 2 * math.pi * (0.01 + 0.037 * k) * t
-        tone = torch.stack([160.0 * torch.cos(ph), 160.0 * torch.sin(ph)], -1)  # [h][s][2]
-        v[:, :, c] += tone[:, None, :, None, :]
+    add_rfi_tones(torch, v, RFI_CHANNELS)
     if pulse:
         freqs = synthetic.channel_frequencies(centre, bwidth, F)
         fref = freqs.max()
@@ -657,6 +667,7 @@ def uhf_case(torch, stages, synthetic, K, W):
                                                 dispatch=[U["idd_dispatch"]] * len(blocks))
     gen = torch.Generator(device="cuda").manual_seed(4321)
     taftp = (torch.randn((T // 256, A, F, 256, 2, 2), generator=gen, device="cuda") * 8.0)
+    add_rfi_tones(torch, taftp, UHF_RFI_CHANNELS)
     taftp = taftp.round_().clamp_(-127, 127).to(torch.int8)
     stream = torch.cuda.current_stream()
 
@@ -684,7 +695,8 @@ def uhf_case(torch, stages, synthetic, K, W):
     adds = sum(U["ntrials"] * (T // ts) * B * F for _ in blocks)
     return {"workload": "UHF 544-1088 MHz (top 256 of 1024 channels), 64 ant x 2048 beams, "
                         "coherent DMs {0,300}, tscrunch 8, 128 incoherent trials per coherent "
-                        "DM over +-50, device aggregation (dispatch 32768)",
+                        "DM over +-50, device aggregation (dispatch 32768); sigma-8 voltages "
+                        "with RFI tones at 20 sigma in channels 40, 130 and 200",
             "ms_per_gulp": ms, "rtf": gulp_s / (ms * 1e-3),
             "idd_adds_per_gulp": adds, "idd_overlap_samples": [g[1] for g in geo],
             "timed_gulps": K, "warmup_gulps": W}
