@@ -122,7 +122,7 @@ def cpu_baseline(threads=None, nsamp=2048):
     dms = WORK["dms"]
     chbw = WORK["chbw"]
     low = WORK["centre"] - 32 * chbw
-    fft_len, ov = 8192, 1472
+    fft_len, ov, lag = O.cdd_plan(WORK["centre"], 64 * chbw, 64, dms)
     ext = np.clip(np.rint(g.normal(0, 8, size=(1, ov + nsamp, 2, A, 2))), -127, 127).astype(np.int8)
     delays = synthetic.delay_model(g, B, A)
     freqs = np.array([low + chbw / 2])
@@ -137,7 +137,7 @@ def cpu_baseline(threads=None, nsamp=2048):
     dd = {}
 
     def cdd_task(d):
-        return d, O.cdd_ftpa(ext, nsamp, chirps[d], ov)
+        return d, O.cdd_ftpa(ext, nsamp, chirps[d], ov, lag=lag)
 
     with cf.ThreadPoolExecutor(threads) as ex:
         for d, v in ex.map(cdd_task, dms):
@@ -174,10 +174,11 @@ def run_reference(args):
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int8", "data": "synthetic",
-            "config": config_block({"inputs": INPUTS + " (the timed CPU sample is a Gaussian "
-                                    "slice: the CPU path's cost does not depend on the values)"}),
-            "cpu_baseline": {k: vals[-1][k] for k in ("kind", "cores", "sample")} | {"value": v,
-                                                                                   "unit": "x real-time"},
+            "config": config_block({"inputs": INPUTS}),
+            "cpu_baseline": {"kind": vals[-1]["kind"], "cores": vals[-1]["cores"],
+                             "sample": vals[-1]["sample"] + " (a Gaussian slice: the CPU path's "
+                                       "cost does not depend on the values)",
+                             "value": v, "unit": "x real-time"},
             "e2e": {"value": v, "unit": "x real-time", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -336,7 +337,7 @@ def main_b200(args):
                   beamset_weights=bwts, beamset_mapping=mapping)
     pipe = stages.BeamformerPipeline(**common, grouped=True, use_graph=True)
     pipe.set_delays(delays, 1.7e9)
-    fft_len, overlap = pipe.fft_plan()
+    fft_len, overlap, lag = pipe.cdd_plan()
     epoch0 = 1.7e9
     gulp_s = T * tsamp()
     stream = torch.cuda.current_stream()
@@ -375,8 +376,11 @@ def main_b200(args):
     del plain
 
     # ---- per-kernel timings (CUDA events on the launching stream)
-    kern = kernel_breakdown(torch, stages, taftp, delays, fft_len, overlap, centre, bwidth,
-                            args.steps)
+    kern = kernel_breakdown(torch, stages, taftp, delays, fft_len, overlap, lag, centre,
+                            bwidth, args.steps)
+    # ---- the plan's deviation from 65536-point (= gulp) windows, the
+    # reference's FFT length
+    plan_dev = cdd_window_deviation(torch, stages, taftp, centre, bwidth, fft_len, overlap, lag)
 
     # ---- ragged (DM x beamset) problems: grouped vs plain
     ragged = ragged_case(torch, stages, synthetic, args.steps)
@@ -426,13 +430,14 @@ def main_b200(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_graph,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int8",
             "data": "synthetic", "impl": "b200",
-            "config": config_block({"fft_len": fft_len, "overlap": overlap, "inputs": INPUTS,
-                                    "parallelism": f"{world} independent subbands"}),
+            "config": config_block({"inputs": INPUTS}),
+            "parallelism": f"{world} independent subbands",
             "int8_tops_pipeline": ops_gulp / (ms_graph * 1e-3) / 1e12,
             "cb_int8_tops": cb["tops"],
             "plain": {"value": gulp_s / (ms_plain * 1e-3) * world, "ms_per_step": ms_plain},
             "batched_vs_plain": ms_plain / ms_graph, "ragged": ragged,
             "kernels": kern, "roofline": roof, "hbm_peak_gbs": hbm_peak, "e2e": e2e,
+            "cdd_plan": plan_dev,
             "gpu_launches": launches * args.steps, "clocks": clocks}
     pipe.close()
     line["long_fft"] = long_fft
@@ -451,7 +456,7 @@ def main_b200(args):
         dist.destroy_process_group()
 
 
-def kernel_breakdown(torch, stages, taftp, delays, fft_len, overlap, centre, bwidth, K):
+def kernel_breakdown(torch, stages, taftp, delays, fft_len, overlap, lag, centre, bwidth, K):
     """Each stage timed standalone with CUDA events over K launches."""
     A, B, F, T, ts = WORK["nant"], WORK["nbeams"], WORK["nchans"], WORK["gulp"], WORK["tscrunch"]
     dms = WORK["dms"]
@@ -478,7 +483,8 @@ def kernel_breakdown(torch, stages, taftp, delays, fft_len, overlap, centre, bwi
     ms = timeit(lambda: stages.statistics(ext, T, overlap))
     out["statistics"] = {"ms": ms, "gbs": vbytes / (ms * 1e-3) / 1e9}
     low = centre - bwidth / 2
-    cdd = stages.CoherentDedisperser(F, A, fft_len, overlap, float(np.float32(low)), bwidth, dms)
+    cdd = stages.CoherentDedisperser(F, A, fft_len, overlap, float(np.float32(low)), bwidth, dms,
+                                     lag=lag)
     outs = [torch.empty((F, 2, A, 2, T), dtype=torch.int8, device="cuda") for _ in dms]
     ms = timeit(lambda: cdd.dedisperse(ext, T, outs))
     nseg = -(-T // (fft_len - overlap))
@@ -512,6 +518,43 @@ def kernel_breakdown(torch, stages, taftp, delays, fft_len, overlap, centre, bwi
     return out
 
 
+def cdd_window_deviation(torch, stages, taftp, centre, bwidth, fft_len, overlap, lag,
+                         chans=(0, 32)):
+    """How far the pipeline's overlap-save plan lies from one with 65536-point
+    windows (the reference's FFT length = its gulp length,
+    CoherentDedisperser.cu:47-57) and the same trims, on two channels of the
+    benchmark gulp (lowest and middle), every DM: the fraction of int8
+    dedispersed values that differ and the largest difference (LSB, int8
+    wrap-aware).  Both plans run on this GPU; the test suite pins each of them
+    to the FP64 oracle at its own geometry.  The reference chirp's phase jump
+    at the bin wrap gives its response 1/n tails, so any two window
+    geometries differ by about this much."""
+    A, F, T = WORK["nant"], WORK["nchans"], WORK["gulp"]
+    dms = WORK["dms"]
+    chbw = bwidth / F
+    low = float(np.float32(centre - bwidth / 2))
+    ext = torch.zeros((F, 2, A, 2, overlap + T), dtype=torch.int8, device="cuda")
+    stages.transpose_fpact(taftp, A, overlap + T, overlap, out=ext)
+    res = {"fft_len": fft_len, "overlap": overlap, "lag": lag, "reference_fft_len": 65536,
+           "channels": list(chans), "per_dm": {}}
+    for dm in dms:
+        fr, mx = [], 0
+        for c in chans:
+            x = ext[c:c + 1].contiguous()
+            o = []
+            for n in (fft_len, 65536):
+                cdd = stages.CoherentDedisperser(1, A, n, overlap, low + c * chbw, chbw, [dm],
+                                                 lag=lag)
+                o.append(cdd.dedisperse(x, T)[0].to(torch.int32))
+            d = (o[0] - o[1]).abs()
+            d = torch.minimum(d, 256 - d)
+            fr.append(float((d > 0).float().mean()))
+            mx = max(mx, int(d.max()))
+        res["per_dm"][str(dm)] = {"mismatch_fraction": float(np.mean(fr)), "max_lsb": mx}
+    torch.cuda.synchronize()
+    return res
+
+
 RAGGED = dict(nant=64, nchans=64, gulp=32768, tscrunch=16, dms=[0.0, 50.0, 150.0, 500.0],
               ants=[64, 57, 48, 40, 32, 24, 16, 8], beams=[512, 256, 256, 128, 128, 64, 64, 32])
 
@@ -526,7 +569,7 @@ def long_fft_case(torch, stages, synthetic, taftp, common, K):
     cfg = dict(common, nbeams=B, beamset_mapping=np.zeros(B, np.int32))
     pipe = stages.BeamformerPipeline(**cfg, fft_len=65536, grouped=True, use_graph=True)
     pipe.set_delays(synthetic.delay_model(synthetic.rng(256), B, cfg["nantennas"]), 1.7e9)
-    fft_len, overlap = pipe.fft_plan()
+    fft_len, overlap, lag = pipe.cdd_plan()
     gulp_s = cfg["gulp_samples"] * tsamp()
     for i in range(3):
         pipe.process_device(taftp, 1.7e9 + i * gulp_s)
@@ -541,8 +584,8 @@ def long_fft_case(torch, stages, synthetic, taftp, common, K):
     pipe.close()
     return {"workload": f"{cfg['nantennas']}ant x {B}beam x {cfg['nchans']}ch x "
                         f"{cfg['gulp_samples']}-sample gulps, DMs {list(cfg['dms'])}, "
-                        f"{fft_len}-point windows (overlap {overlap})",
-            "fft_len": fft_len, "overlap": overlap, "ms_per_gulp": ms,
+                        f"{fft_len}-point windows (overlap {overlap}, lag {lag})",
+            "fft_len": fft_len, "overlap": overlap, "lag": lag, "ms_per_gulp": ms,
             "rtf": gulp_s / (ms * 1e-3), "timed_gulps": K, "warmup_gulps": 3}
 
 
@@ -767,11 +810,12 @@ def profile_case(which, nchans=16, reps=3):
         fn = lambda: stages.coherent_beamform_grouped([(fp, out, ib, 0, B)], gemm, scl, scl,
                                                       mapping, T, ts)
     else:
-        ov, n = 1472, 8192
+        n, ov, lag = stages.cdd_plan(WORK["centre"], 64 * WORK["chbw"], 64, WORK["dms"])
         ext = torch.zeros((F, 2, A, 2, ov + T), dtype=torch.int8, device="cuda")
         ext[..., ov:] = fp
         low = WORK["centre"] - 32 * WORK["chbw"]
-        cdd = stages.CoherentDedisperser(F, A, n, ov, low, F * WORK["chbw"], WORK["dms"])
+        cdd = stages.CoherentDedisperser(F, A, n, ov, low, F * WORK["chbw"], WORK["dms"],
+                                         lag=lag)
         outs = [torch.empty((F, 2, A, 2, T), dtype=torch.int8, device="cuda") for _ in WORK["dms"]]
         fn = lambda: cdd.dedisperse(ext, T, outs)
     for _ in range(1 + reps):

@@ -129,8 +129,10 @@ int sw_statistics(const void* d_fpact, size_t row_stride, size_t sample_offset,
  *   - at most 16384 (channel, pol, antenna) series; larger shapes return
  *     SW_ERR_INVALID with a message, nothing is launched;
  *   - the first call on each device looks up the array's device address
- *     (cudaGetSymbolAddress with that device current); make that first call
- *     before capturing any stream;
+ *     (cudaGetSymbolAddress with that device current) and keeps it for the
+ *     process; make that first call before capturing any stream.  A
+ *     cudaDeviceReset invalidates the kept address, so do not call this
+ *     entry point on a device after resetting it;
  *   - every call shares the one array (it is cleared at the start of each
  *     call): calls whose kernels overlap on the GPU, from any stream or
  *     thread, race and give wrong statistics;
@@ -142,8 +144,8 @@ int sw_statistics_noalloc(const void* d_fpact, size_t row_stride,
 /* Replaces StatisticsCalculator::update_scalings
  * (cpp/skyweaver/StatisticsCalculator.cuh:96-97,
  *  cpp/skyweaver/src/StatisticsCalculator.cu:132-239), computed on the
- * device.  Outputs are indexed [beamset*nchans + chan] (the reference writes
- * [chan] for every beamset). */
+ * device.  Outputs are indexed [beamset*nchans + chan]: the reference writes
+ * [chan] for every beamset, which leaves beamsets above 0 with scale 0. */
 int sw_update_scalings(const float* d_stats, const float* d_beamset_weights,
                        int nbeamsets, int nchans, int npol, int nant,
                        int cb_tscrunch, int ib_tscrunch, float output_level,
@@ -245,18 +247,36 @@ int sw_cdd_chirps(const float* h_dms, int ndms, int nchans, int fft_len,
                   double low_freq, double bw, void* d_setup,
                   sw_stream_t stream);
 
+/* The overlap-save plan, host only (replaces the overlap and FFT-length
+ * choice of create_coherent_dedisperser_config,
+ * cpp/skyweaver/src/CoherentDedisperser.cu:19-57, which sizes the overlap by
+ * the whole subband's DM delay and takes the gulp as the FFT length).  Each
+ * window trims, at its start, the largest intra-channel DM smear (lowest
+ * channel, largest DM) rounded up to 16 samples and, at its end, `*lag`
+ * samples (lag_request rounded up to 16; 0 = 128): *overlap is their sum.
+ * *fft_len > 0 on entry is kept if it exceeds the overlap; 0 picks one by a
+ * cost model (on-chip sizes up to 8192 first).  SW_ERR_INVALID if none fits. */
+int sw_cdd_plan(double centre_frequency, double bandwidth, int nchans,
+                const float* h_dms, int ndms, int lag_request, int* fft_len,
+                int* overlap, int* lag);
+
 /* Replaces CoherentDedisperser::dedisperse
  * (cpp/skyweaver/CoherentDedisperser.cuh:77-80,
  *  cpp/skyweaver/src/CoherentDedisperser.cu:142-225) for all channels,
  * antennas, pols and DMs of a gulp with correct overlap-save: input rows
  * hold `overlap` history samples then nsamples new samples
- * (row_stride >= overlap + nsamples); output d_out[dm] is FPACT with
- * row stride out_row_stride holding nsamples samples delayed by overlap/2.
- * Requantisation wraps to int8 like the reference. */
+ * (row_stride >= overlap + nsamples); every fft_len-point window advances by
+ * fft_len - overlap samples and trims overlap - lag samples at its start and
+ * lag at its end, so output d_out[dm] (FPACT, row stride out_row_stride)
+ * holds nsamples samples delayed by `lag` (0 <= lag <= overlap).  The
+ * reference trims overlap/2 at each end (lag = overlap / 2); its chirp's
+ * response lies almost entirely at causal lags up to the intra-channel smear,
+ * so a plan with overlap - lag >= that smear and a small lag is wrap-free at
+ * a smaller overlap.  Requantisation wraps to int8 like the reference. */
 int sw_coherent_dedisperse(const void* d_fpact_in, size_t row_stride,
                            int nchans, int npol, int nant, int nsamples,
-                           int fft_len, int overlap, const void* d_setup,
-                           int ndms, void* const* h_d_out,
+                           int fft_len, int overlap, int lag,
+                           const void* d_setup, int ndms, void* const* h_d_out,
                            size_t out_row_stride, sw_stream_t stream);
 
 /* Workspace bytes sw_coherent_dedisperse_ws needs to process every
@@ -274,7 +294,8 @@ size_t sw_cdd_workspace_bytes(int nchans, int npol, int nant, int nsamples,
  * [nsamples] (re, im), for precision studies against an FP64 reference. */
 int sw_coherent_dedisperse_ws(const void* d_fpact_in, size_t row_stride,
                               int nchans, int npol, int nant, int nsamples,
-                              int fft_len, int overlap, const void* d_setup,
+                              int fft_len, int overlap, int lag,
+                              const void* d_setup,
                               int ndms, void* const* h_d_out,
                               size_t out_row_stride, void* d_workspace,
                               size_t workspace_bytes, float* d_debug_f32,
@@ -343,6 +364,7 @@ int sw_idd_pipeline_geometry(const sw_idd_pipeline* p, int block,
 typedef struct sw_tuning {
     int fft_len;            /* coherent dedispersion FFT length          */
     int overlap;            /* overlap-save overlap (samples)            */
+    int lag;                /* of it, trimmed at each window's end       */
     int cb_tiles_per_item;  /* sw_cb_shape.tiles_per_item                */
     float cdd_ms, cb_ms;    /* measured per gulp at the chosen settings  */
 } sw_tuning;
@@ -438,6 +460,10 @@ typedef struct sw_pipeline_config {
     const int* beamset_mapping;   /* host [nbeams]                       */
     int autotune;           /* 1 = sw_autotune picks fft_len (if 0) and the
                                beamformer work-item size                 */
+    int cdd_lag;            /* coherent dedispersion: samples trimmed at the
+                               end of each window, i.e. the output delay
+                               (0 = 128); the start trim is the largest
+                               intra-channel DM smear rounded up to 16   */
 } sw_pipeline_config;
 
 int sw_pipeline_create(const sw_pipeline_config* cfg, sw_pipeline** out);
@@ -457,8 +483,19 @@ int sw_pipeline_process_host(sw_pipeline* p, const void* h_taftp,
 int sw_pipeline_outputs(sw_pipeline* p, int dm_idx, const int8_t** d_cb_tfb,
                         const float** d_ib_raw, const int8_t** d_ib_btf,
                         const float** d_stats);
+/* The last gulp's voltages that fed the beamformers for one DM: the
+ * dedispersed FPACT rows (nsamples of the gulp from the row start, delayed
+ * by the plan's lag), or the transposed gulp without coherent dedispersion
+ * (the reference pipeline's _ftpa_dedispersed, detail/BeamformerPipeline.cu:
+ * 190-205).  Valid until the next gulp is processed. */
+int sw_pipeline_voltages(sw_pipeline* p, int dm_idx, const int8_t** d_fpact,
+                         size_t* row_stride);
 size_t sw_pipeline_cb_bytes_per_dm(const sw_pipeline* p);
-int sw_pipeline_fft_len(const sw_pipeline* p, int* fft_len, int* overlap);
+/* The coherent-dedispersion plan: FFT length, overlap (history samples) and
+ * lag (trim at each window's end = delay of the dedispersed output; the
+ * outputs' utc_offset is lag / channel bandwidth).  Any pointer may be NULL. */
+int sw_pipeline_fft_len(const sw_pipeline* p, int* fft_len, int* overlap,
+                        int* lag);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

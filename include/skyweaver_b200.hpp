@@ -892,13 +892,15 @@ class BeamformerPipeline {
     {
         if(dm_idx >= _config.coherent_dms().size())
             throw std::runtime_error("BeamformerPipeline: DM index out of range");
-        int fft_len = 0, overlap = 0;
-        check(sw_pipeline_fft_len(_p, &fft_len, &overlap));
+        int fft_len = 0, overlap = 0, lag = 0;
+        check(sw_pipeline_fft_len(_p, &fft_len, &overlap, &lag));
         const double chan_tsamp = (double)_config.nchans() / _config.bandwidth();
         Description d;
         d.freqs         = _config.channel_frequencies();
         d.sample_period = chan_tsamp;
-        d.offset        = chan_tsamp * overlap / 2.0;  // CoherentDedisperser.cu:82
+        // the filter delay (CoherentDedisperser.cu:82 sets tsamp * overlap / 2
+        // for its symmetric trim): the samples trimmed at each window's end
+        d.offset        = chan_tsamp * lag;
         d.coherent_dm   = _config.coherent_dms()[dm_idx];
         return d;
     }

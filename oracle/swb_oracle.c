@@ -387,9 +387,12 @@ static void fft64(double* x, int n, int sign)
 /* ------------------------------------------------------------------ */
 /* One overlap-save segment of coherent dedispersion for one stream:    */
 /* CoherentDedisperser.cu:142-225 (int8 -> complex, FFT, chirp multiply,*/
-/* inverse FFT, trim overlap/2 each side, /N, round, int8 wrap) with    */
-/* the FP64 arithmetic of dedisperse.py:159-164 (complex128 FFT,        */
-/* complex64 cast of the normalised result, round-half-even, int8 cast).*/
+/* inverse FFT, trim the overlap, /N, round, int8 wrap) with the FP64   */
+/* arithmetic of dedisperse.py:159-164 (complex128 FFT, complex64 cast  */
+/* of the normalised result, round-half-even, int8 cast).               */
+/* The reference trims overlap/2 samples at each end of the window      */
+/* (:196-223); here `lag` samples are trimmed at the end and            */
+/* overlap - lag at the start, so lag = overlap / 2 is the reference.   */
 /*   in:   int8 char2 [fft_len] (a zero-padded window of the stream)    */
 /*   chirp: complex double [fft_len]                                    */
 /*   out_i8: char2 [fft_len - overlap]                                  */
@@ -397,8 +400,8 @@ static void fft64(double* x, int n, int sign)
 /*            dedispersed voltages before requantisation                */
 /* ------------------------------------------------------------------ */
 SWO_EXPORT void swo_cdd_segment(const int8_t* in, const double* chirp,
-                                int fft_len, int overlap, int8_t* out_i8,
-                                double* out_f64)
+                                int fft_len, int overlap, int lag,
+                                int8_t* out_i8, double* out_f64)
 {
     double* x = (double*)malloc(sizeof(double) * 2 * (size_t)fft_len);
     for(int i = 0; i < fft_len; ++i) {
@@ -413,9 +416,9 @@ SWO_EXPORT void swo_cdd_segment(const int8_t* in, const double* chirp,
         x[2 * k + 1] = a * d + b * c;
     }
     fft64(x, fft_len, +1);
-    int half = overlap / 2;
+    int head = overlap - lag;
     for(int i = 0; i < fft_len - overlap; ++i) {
-        double re = x[2 * (i + half)] / fft_len, im = x[2 * (i + half) + 1] / fft_len;
+        double re = x[2 * (i + head)] / fft_len, im = x[2 * (i + head) + 1] / fft_len;
         if(out_f64) {
             out_f64[2 * i]     = re;
             out_f64[2 * i + 1] = im;
@@ -433,14 +436,14 @@ SWO_EXPORT void swo_cdd_segment(const int8_t* in, const double* chirp,
 /*   stream: char2 [overlap + nsamples] = history (overlap samples of  */
 /*           the previous gulp, zeros for the first gulp) + this gulp   */
 /*   out:    char2 [nsamples]; out[m] is the dedispersed voltage at     */
-/*           input position m - overlap/2 relative to this gulp start   */
+/*           input position m - lag relative to this gulp start         */
 /*   Segment k takes input [k*L, k*L + fft_len) of `stream`, zero       */
 /*   padded past the end, and yields outputs [k*L, k*L + L) with        */
 /*   L = fft_len - overlap.                                             */
 /* ------------------------------------------------------------------ */
 SWO_EXPORT void swo_cdd_stream(const int8_t* stream, int nsamples,
                                const double* chirp, int fft_len, int overlap,
-                               int8_t* out, double* out_f64)
+                               int lag, int8_t* out, double* out_f64)
 {
     int L = fft_len - overlap;
     int8_t* seg = (int8_t*)malloc(2 * (size_t)fft_len);
@@ -454,7 +457,7 @@ SWO_EXPORT void swo_cdd_stream(const int8_t* stream, int nsamples,
             seg[2 * i]     = src < total ? stream[2 * src] : 0;
             seg[2 * i + 1] = src < total ? stream[2 * src + 1] : 0;
         }
-        swo_cdd_segment(seg, chirp, fft_len, overlap, so, sf);
+        swo_cdd_segment(seg, chirp, fft_len, overlap, lag, so, sf);
         int n = nsamples - start < L ? nsamples - start : L;
         memcpy(out + 2 * (size_t)start, so, 2 * (size_t)n);
         if(out_f64) memcpy(out_f64 + 2 * (size_t)start, sf, sizeof(double) * 2 * (size_t)n);

@@ -175,31 +175,41 @@ def chirp(nchans, fft_len, low_freq, bw, dm):
     return out
 
 
-def cdd_segment(stream, chirp_row, overlap, want_f64=False):
+def cdd_segment(stream, chirp_row, overlap, want_f64=False, lag=None):
     """One FFT -> chirp -> IFFT -> trim -> /N -> round -> int8-wrap segment.
-    stream: int8 [fft_len][2]; chirp_row: complex128 [fft_len]."""
+    stream: int8 [fft_len][2]; chirp_row: complex128 [fft_len].  `lag`
+    samples are trimmed at the end of the window and overlap - lag at its
+    start; None is the reference's overlap / 2 at each end
+    (CoherentDedisperser.cu:196-223)."""
     stream = _c(stream, np.int8)
     n = stream.shape[0]
+    lag = overlap // 2 if lag is None else int(lag)
+    if not 0 <= lag <= overlap:
+        raise ValueError("lag must lie in [0, overlap]")
     ch = _c(chirp_row, np.complex128)
     out = np.empty((n - overlap, 2), np.int8)
     f64 = np.empty(n - overlap, np.complex128) if want_f64 else None
-    lib().swo_cdd_segment(_p(stream), _p(ch), n, overlap, _p(out), _p(f64))
+    lib().swo_cdd_segment(_p(stream), _p(ch), n, overlap, lag, _p(out), _p(f64))
     return (out, f64) if want_f64 else out
 
 
-def cdd_stream(stream, nsamples, chirp_row, overlap, want_f64=False):
+def cdd_stream(stream, nsamples, chirp_row, overlap, want_f64=False, lag=None):
     """Overlap-save over a gulp for one stream: stream int8 [overlap+T][2]
-    (history then gulp) -> int8 [T][2] (and FP64 values [T])."""
+    (history then gulp) -> int8 [T][2] (and FP64 values [T]); output m is
+    the dedispersed voltage at gulp position m - lag."""
     stream = _c(stream, np.int8)
+    lag = overlap // 2 if lag is None else int(lag)
+    if not 0 <= lag <= overlap:
+        raise ValueError("lag must lie in [0, overlap]")
     ch = _c(chirp_row, np.complex128)
     out = np.empty((nsamples, 2), np.int8)
     f64 = np.empty(nsamples, np.complex128) if want_f64 else None
-    lib().swo_cdd_stream(_p(stream), nsamples, _p(ch), len(ch), overlap,
+    lib().swo_cdd_stream(_p(stream), nsamples, _p(ch), len(ch), overlap, lag,
                          _p(out), _p(f64))
     return (out, f64) if want_f64 else out
 
 
-def cdd_ftpa(ftpa_ext, nsamples, chirps, overlap, want_f64=False):
+def cdd_ftpa(ftpa_ext, nsamples, chirps, overlap, want_f64=False, lag=None):
     """Coherent dedispersion of a whole FTPA gulp for one DM.
     ftpa_ext: int8 [F][overlap+T][P][A][2] (history + gulp);
     chirps: complex128 [F][fft_len].  Returns int8 FTPA [F][T][P][A][2]."""
@@ -210,12 +220,41 @@ def cdd_ftpa(ftpa_ext, nsamples, chirps, overlap, want_f64=False):
         for p in range(P):
             for a in range(A):
                 r = cdd_stream(ftpa_ext[f, :, p, a], nsamples, chirps[f], overlap,
-                               want_f64)
+                               want_f64, lag)
                 if want_f64:
                     out[f, :, p, a], f64[f, :, p, a] = r
                 else:
                     out[f, :, p, a] = r
     return (out, f64) if want_f64 else out
+
+
+def cdd_plan(centre_frequency, bandwidth, nchans, dms, fft_len=0, lag=128):
+    """The pipeline's overlap-save plan restated: (fft_len, overlap, lag).
+
+    The reference's chirp (CoherentDedisperser.cu:313-335) has a one-sided
+    impulse response: nearly all of it lies at lags 0 .. the intra-channel
+    smear of the lowest channel at the largest DM.  The window therefore
+    trims that smear (rounded up to 16) at its start and a margin `lag`
+    (rounded up to 16) at its end, which holds the response's short
+    anti-causal part; the output is delayed by `lag` samples."""
+    chbw = bandwidth / nchans
+    f_low = float(np.float32(centre_frequency - bandwidth / 2.0))
+    smear = 4.148806423e15 * (1.0 / f_low ** 2 - 1.0 / (f_low + chbw) ** 2) * max(dms)
+    head = (int(np.ceil(smear * chbw)) + 15) // 16 * 16
+    lag = (int(lag) + 15) // 16 * 16
+    overlap = head + lag
+    if not fft_len:
+        best = None
+        for n in (1024, 2048, 4096, 8192):
+            if n <= overlap:
+                continue
+            cost = np.log2(n) / (1.0 - overlap / n)
+            if best is None or cost < best[0] - 1e-9:
+                best = (cost, n)
+        if best is None:
+            best = (0.0, next(n for n in (16384, 32768, 65536) if n > overlap))
+        fft_len = best[1]
+    return fft_len, overlap, lag
 
 
 # -------------------------------------------------------- incoherent dedisp.

@@ -51,11 +51,11 @@ class PipelineConfig(ctypes.Structure):
                 ("enable_coherent_dedispersion", c_int), ("grouped", c_int),
                 ("use_graph", c_int), ("nbeamsets", c_int),
                 ("beamset_weights", c_float_p), ("beamset_mapping", ctypes.POINTER(c_int)),
-                ("autotune", c_int)]
+                ("autotune", c_int), ("cdd_lag", c_int)]
 
 
 class Tuning(ctypes.Structure):
-    _fields_ = [("fft_len", c_int), ("overlap", c_int), ("cb_tiles_per_item", c_int),
+    _fields_ = [("fft_len", c_int), ("overlap", c_int), ("lag", c_int), ("cb_tiles_per_item", c_int),
                 ("cdd_ms", c_float), ("cb_ms", c_float)]
 
 
@@ -97,11 +97,11 @@ _SIGS = {
     "sw_cdd_chirps": (c_int, [c_float_p, c_int, c_int, c_int, c_double, c_double, c_void_p,
                               c_void_p]),
     "sw_coherent_dedisperse": (c_int, [c_void_p, c_size_t, c_int, c_int, c_int, c_int, c_int,
-                                       c_int, c_void_p, c_int, ctypes.POINTER(c_void_p),
+                                       c_int, c_int, c_void_p, c_int, ctypes.POINTER(c_void_p),
                                        c_size_t, c_void_p]),
     "sw_cdd_workspace_bytes": (c_size_t, [c_int, c_int, c_int, c_int, c_int, c_int, c_int]),
     "sw_coherent_dedisperse_ws": (c_int, [c_void_p, c_size_t, c_int, c_int, c_int, c_int, c_int,
-                                          c_int, c_void_p, c_int, ctypes.POINTER(c_void_p),
+                                          c_int, c_int, c_void_p, c_int, ctypes.POINTER(c_void_p),
                                           c_size_t, c_void_p, c_size_t, c_void_p, c_void_p]),
     "sw_idd_pipeline_create": (c_int, [c_int, c_int, c_int, ctypes.POINTER(c_int),
                                        ctypes.POINTER(c_void_p), ctypes.POINTER(c_int),
@@ -125,7 +125,12 @@ _SIGS = {
                                     ctypes.POINTER(c_void_p), ctypes.POINTER(c_void_p),
                                     ctypes.POINTER(c_void_p)]),
     "sw_pipeline_cb_bytes_per_dm": (c_size_t, [c_void_p]),
-    "sw_pipeline_fft_len": (c_int, [c_void_p, ctypes.POINTER(c_int), ctypes.POINTER(c_int)]),
+    "sw_cdd_plan": (c_int, [c_double, c_double, c_int, c_float_p, c_int, c_int,
+                            ctypes.POINTER(c_int), ctypes.POINTER(c_int), ctypes.POINTER(c_int)]),
+    "sw_pipeline_voltages": (c_int, [c_void_p, c_int, ctypes.POINTER(c_void_p),
+                                     ctypes.POINTER(c_size_t)]),
+    "sw_pipeline_fft_len": (c_int, [c_void_p, ctypes.POINTER(c_int), ctypes.POINTER(c_int),
+                                    ctypes.POINTER(c_int)]),
 }
 
 _lib = None

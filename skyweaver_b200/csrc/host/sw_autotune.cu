@@ -80,7 +80,9 @@ extern "C" int sw_autotune(int nantennas, int nbeams, int nchans, int nsamples, 
                "sw_autotune: nantennas must be 16, 32 or 64");
     SW_REQUIRE(nchans > 0 && nbeams > 0 && nsamples > 0 && nsamples % 64 == 0 && tscrunch > 0,
                "sw_autotune: bad shape");
-    const int overlap = cdd_overlap(centre_frequency, bandwidth, nchans, h_dms, ndms);
+    // the pipeline's default overlap-save plan (sw_host.hpp)
+    const int lag     = cdd_round_lag(0);
+    const int overlap = cdd_head(centre_frequency, bandwidth, nchans, h_dms, ndms) + lag;
     const Key key{nantennas, nbeams, nchans, nsamples, tscrunch, ndms, overlap};
     {
         std::lock_guard<std::mutex> lk(g_mu);
@@ -106,6 +108,7 @@ extern "C" int sw_autotune(int nantennas, int nbeams, int nchans, int nsamples, 
     // (on-chip sizes when any fits, the split sizes otherwise)
     sw_tuning best{};
     best.overlap = overlap;
+    best.lag     = lag;
     best.cdd_ms = 1e30f;
     std::vector<int> lens;
     for(int n = 1024; n <= 8192; n *= 2)
@@ -133,7 +136,7 @@ extern "C" int sw_autotune(int nantennas, int nbeams, int nchans, int nsamples, 
                                : 0;
         float ms = 0.0f;
         SW_TRY(time_ms([&] {
-            return sw_coherent_dedisperse_ws(in.p, stride, F, 2, A, T, n, overlap, st.p, ndm,
+            return sw_coherent_dedisperse_ws(in.p, stride, F, 2, A, T, n, overlap, lag, st.p, ndm,
                                              dd.data(), (size_t)T, wsn ? ws.p : nullptr, wsn,
                                              nullptr, stream);
         }, s, 3, &ms));

@@ -8,11 +8,18 @@ namespace swb {
 
 constexpr double kDmConst = 4.148806423e15;  // dedispersion_utils.cuh:12-13
 
-// Overlap-save overlap of the coherent dedisperser: the largest intra-channel
-// DM smear (lowest channel, largest DM) in samples, rounded up to a multiple
-// of 16 so that every segment start stays 16-byte aligned.
-inline int cdd_overlap(double centre_frequency, double bandwidth, int nchans, const float* dms,
-                       int ndms)
+// Overlap-save plan of the coherent dedisperser.  The reference's chirp
+// (CoherentDedisperser.cu:313-335) has a one-sided impulse response: nearly
+// all of it lies at causal lags up to the intra-channel DM smear of the lowest
+// channel at the largest DM.  A window therefore trims that smear, rounded up
+// to a multiple of 16, at its start (`head`) and `lag` samples (default 128,
+// rounded up to 16) at its end, which hold the response's short anti-causal
+// part; overlap = head + lag and the output is delayed by lag samples.
+// Multiples of 16 keep every window start 16-byte aligned.
+constexpr int kCddDefaultLag = 128;
+
+inline int cdd_head(double centre_frequency, double bandwidth, int nchans, const float* dms,
+                    int ndms)
 {
     const double chbw = bandwidth / nchans;
     const float f_low = (float)(centre_frequency - bandwidth / 2.0f);
@@ -25,8 +32,11 @@ inline int cdd_overlap(double centre_frequency, double bandwidth, int nchans, co
     return (ov + 15) / 16 * 16;
 }
 
+inline int cdd_round_lag(int lag) { return ((lag > 0 ? lag : kCddDefaultLag) + 15) / 16 * 16; }
+
 // FFT length by a cost model (log2 N operations per sample over the useful
-// fraction 1 - overlap / N), on-chip sizes only; 0 if none fits.
+// fraction 1 - overlap / N), on-chip sizes (<= 8192) when one exceeds the
+// overlap, else the smallest split size (16384 .. 65536) that does; 0 if none.
 inline int cdd_model_fft_len(int overlap)
 {
     int fft_len = 0;
@@ -36,6 +46,8 @@ inline int cdd_model_fft_len(int overlap)
         const double cost = std::log2((double)n) / (1.0 - (double)overlap / n);
         if(cost < best - 1e-9) { best = cost; fft_len = n; }
     }
+    for(int n = 16384; fft_len == 0 && n <= 65536; n *= 2)
+        if(n > overlap) fft_len = n;
     return fft_len;
 }
 

@@ -71,6 +71,7 @@ struct sw_pipeline {
     std::vector<double> freqs;
     int nheaps = 0, T = 0, F = 0, A = 0, B = 0, S = 0, ndm = 0, ts = 0;
     int fft_len = 0, overlap = 0;  // overlap: multiple of 16
+    int lag = 0;                   // of it, trimmed at each window's end
     int cb_tpi = 0;                // CB work-item size (0: kernel default)
     size_t ext_stride = 0, ext_off = 0, dd_stride = 0;
     size_t nrows = 0;  // F * P * A * 2
@@ -143,10 +144,12 @@ int sw_pipeline::init(const sw_pipeline_config& c)
     const double fbottom = c.centre_frequency - c.bandwidth / 2.0;
     for(int i = 0; i < F; ++i) freqs.push_back(fbottom + chbw / 2.0 + chbw * i);
 
-    // Coherent dedispersion plan: overlap = largest intra-channel DM smear
-    // (lowest channel, largest DM), rounded up to a multiple of 16.
+    // Coherent dedispersion plan: each window trims the largest intra-channel
+    // DM smear (lowest channel, largest DM) at its start and `lag` samples at
+    // its end; overlap = both, multiples of 16.
     if(c.enable_coherent_dedispersion) {
-        overlap = swb::cdd_overlap(c.centre_frequency, c.bandwidth, F, dms.data(), ndm);
+        lag     = swb::cdd_round_lag(c.cdd_lag);
+        overlap = swb::cdd_head(c.centre_frequency, c.bandwidth, F, dms.data(), ndm) + lag;
         if(c.fft_len > 0) {
             fft_len = c.fft_len;
         } else if(c.autotune) {
@@ -164,6 +167,7 @@ int sw_pipeline::init(const sw_pipeline_config& c)
         SW_REQUIRE(T >= overlap, "pipeline: gulp shorter than the dedispersion overlap");
     } else {
         overlap = 0;
+        lag     = 0;
         fft_len = 0;
     }
     ext_off    = (size_t)overlap;
@@ -259,7 +263,7 @@ int sw_pipeline::enqueue_chain(const void* d_in, int parity, bool first)
     if(cfg.enable_coherent_dedispersion) {
         std::vector<void*> outs(ndm);
         for(int d = 0; d < ndm; ++d) outs[d] = dd[d].p;
-        SW_TRY(sw_coherent_dedisperse_ws(ext.p, ext_stride, F, 2, A, T, fft_len, overlap,
+        SW_TRY(sw_coherent_dedisperse_ws(ext.p, ext_stride, F, 2, A, T, fft_len, overlap, lag,
                                          d_setup.p, ndm, outs.data(), dd_stride, cdd_ws.p,
                                          cdd_ws.n, nullptr, ss));
         SW_TRY(sw_fpact_keep_history(ext.p, nrows, ext_stride, (size_t)overlap, ss));
@@ -318,6 +322,11 @@ int sw_pipeline::run(const void* d_in, int parity, double epoch)
 {
     SW_REQUIRE(have_delays, "pipeline: no delay model set (sw_pipeline_set_delays)");
     last_par = parity;
+    // The chain's first node copies this parity's epoch slot when it runs on
+    // the device.  The previous gulp of the same parity must have done so
+    // before the slot is overwritten, so the host waits for that gulp (a
+    // no-op unless the caller runs more than one gulp ahead of the GPU).
+    SW_CUDA_CHECK(cudaEventSynchronize(comp_done[parity]));
     h_epochs[2 * parity + 0] = epoch;
     h_epochs[2 * parity + 1] = delay_epoch;
     if(!scalings_done || !cfg.use_graph) {
@@ -346,6 +355,23 @@ int sw_pipeline::run(const void* d_in, int parity, double epoch)
 using namespace swb;
 
 extern "C" {
+
+int sw_cdd_plan(double centre_frequency, double bandwidth, int nchans, const float* h_dms,
+                int ndms, int lag_request, int* fft_len, int* overlap, int* lag)
+{
+    SW_REQUIRE(h_dms && ndms > 0 && nchans > 0 && bandwidth > 0.0 && fft_len && overlap && lag,
+               "sw_cdd_plan: bad arguments");
+    const int lg = cdd_round_lag(lag_request);
+    const int ov = cdd_head(centre_frequency, bandwidth, nchans, h_dms, ndms) + lg;
+    int n = *fft_len > 0 ? *fft_len : cdd_model_fft_len(ov);
+    SW_REQUIRE(n > ov && n >= 256 && n <= 65536 && (n & (n - 1)) == 0,
+               "coherent dedispersion: no power-of-two FFT length in [256, 65536] exceeds the "
+               "overlap of %d samples (requested %d)", ov, *fft_len);
+    *fft_len = n;
+    *overlap = ov;
+    *lag     = lg;
+    return SW_OK;
+}
 
 int sw_pipeline_create(const sw_pipeline_config* cfg, sw_pipeline** out)
 {
@@ -439,13 +465,28 @@ int sw_pipeline_outputs(sw_pipeline* p, int dm_idx, const int8_t** d_cb_tfb,
     return SW_OK;
 }
 
+int sw_pipeline_voltages(sw_pipeline* p, int dm_idx, const int8_t** d_fpact, size_t* row_stride)
+{
+    SW_REQUIRE(p && dm_idx >= 0 && dm_idx < p->ndm && d_fpact && row_stride,
+               "sw_pipeline_voltages: bad arguments");
+    if(p->cfg.enable_coherent_dedispersion) {
+        *d_fpact    = p->dd[dm_idx].as<int8_t>();
+        *row_stride = p->dd_stride;
+    } else {
+        *d_fpact    = p->ext.as<int8_t>() + p->ext_off;
+        *row_stride = p->ext_stride;
+    }
+    return SW_OK;
+}
+
 size_t sw_pipeline_cb_bytes_per_dm(const sw_pipeline* p) { return p ? p->cb_bytes() : 0; }
 
-int sw_pipeline_fft_len(const sw_pipeline* p, int* fft_len, int* overlap)
+int sw_pipeline_fft_len(const sw_pipeline* p, int* fft_len, int* overlap, int* lag)
 {
     SW_REQUIRE(p, "sw_pipeline_fft_len: null pipeline");
     if(fft_len) *fft_len = p->fft_len;
     if(overlap) *overlap = p->overlap;
+    if(lag) *lag = p->lag;
     return SW_OK;
 }
 

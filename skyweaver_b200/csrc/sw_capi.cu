@@ -22,14 +22,15 @@ const char* last_error() { return t_last_error.c_str(); }
 
 __device__ int g_device_error = 0;
 
+// Device address of g_device_error on the current device.  Every device that
+// loads the library has its own copy, so the address is looked up on each
+// launch (a runtime table lookup) instead of cached: a cache would hand one
+// device's address to kernels on another, or go stale after cudaDeviceReset.
 int* device_error_ptr()
 {
-    static int* ptr = nullptr;
-    if(ptr == nullptr) {
-        void* p = nullptr;
-        if(cudaGetSymbolAddress(&p, g_device_error) == cudaSuccess) ptr = static_cast<int*>(p);
-    }
-    return ptr;
+    void* p = nullptr;
+    return cudaGetSymbolAddress(&p, g_device_error) == cudaSuccess ? static_cast<int*>(p)
+                                                                   : nullptr;
 }
 
 }  // namespace swb

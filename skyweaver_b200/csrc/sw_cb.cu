@@ -868,6 +868,7 @@ int launch(const sw_cb_shape* s, const sw_cb_problem* probs, int nprob,
     P.mapping = mapping;
     P.debug   = debug;
     P.err     = device_error_ptr();
+    SW_REQUIRE(P.err != nullptr, "coherent beamformer: the device error word has no address");
     // kind::i8 instruction descriptor: D=S32, A=B=S8, A K-major, B MN-major,
     // N=128 (bits 17-22: N>>3), M=128 (bits 24-28: M>>4)
     P.idesc = (2u << 4) | (1u << 7) | (1u << 10) | (0u << 15) | (1u << 16) |

@@ -19,6 +19,13 @@
 //     int8-wrapped samples straight to the planar output rows.
 // So the forward transform is done once per segment for all DMs, there is
 // no spectrum in HBM, and all global traffic is coalesced byte rows.
+//
+// Trim.  The reference trims overlap/2 samples at each end of a window.  Its
+// chirp's impulse response is one-sided (nearly all of it at lags 0 .. the
+// intra-channel smear), so a window here trims `overlap - lag` samples at its
+// start (the causal part) and `lag` at its end (the short anti-causal part);
+// output sample m is the dedispersed voltage at gulp position m - lag.
+// lag = overlap / 2 is the reference's own per-window trim.
 // Twiddles come from per-pass tables (FP64-computed) staged in shared
 // memory; FFT arithmetic is FP32.
 #include <algorithm>
@@ -216,7 +223,8 @@ struct Args {
     size_t row_stride;
     int nstreams;      // F * P * A
     int nsamples;      // T
-    int overlap;       // O (even)
+    int overlap;       // O: samples of history in front of the gulp
+    int lag;           // trimmed at the end of each window (output delay)
     int nseg;
     int ndms;
     const c32* tw;     // twiddle tables
@@ -366,7 +374,7 @@ cdd_kernel(const __grid_constant__ Args A)
     for(int i = threadIdx.x; i < P.tw_total; i += NT) tw_s[i] = A.tw[i];
 
     const int L = N - A.overlap;
-    const int half = A.overlap / 2;
+    const int head = A.overlap - A.lag;  // trimmed at the start of each window
     const float inv_n = 1.0f / (float)N;  // exact (power of two)
     const int nitems = A.nstreams * A.nseg;
     const bool aligned = (A.row_stride % 16 == 0) && (L % 16 == 0) &&
@@ -468,8 +476,8 @@ cdd_kernel(const __grid_constant__ Args A)
 #pragma unroll
                 for(int r = 0; r < R0; ++r) {
                     const int i = j + r * s0;           // index within the window
-                    const int m = start + i - half;     // output sample in the gulp
-                    if(i >= half && i < half + L && m < A.nsamples) {
+                    const int m = start + i - head;     // output sample in the gulp
+                    if(i >= head && i < head + L && m < A.nsamples) {
                         const float fr = z[r].x * inv_n, fi = z[r].y * inv_n;
                         o_re[m] = (uint8_t)__float2int_rn(fr);  // int8 wrap, like static_cast<char>
                         o_im[m] = (uint8_t)__float2int_rn(fi);
@@ -504,7 +512,7 @@ constexpr int kSplitM   = 1 << kSplitLog;
 struct SplitArgs {
     const uint8_t* in;
     size_t row_stride;
-    int nstreams, nsamples, overlap, nseg, ndms, npa;
+    int nstreams, nsamples, overlap, lag, nseg, ndms, npa;
     int item0, nitems;  // work items [item0, item0 + nitems) of this chunk
     const c32* tw;      // M-point plan tables
     const c32* chirp;   // [ndms][F][S][M]: bin k1 + S k2 at k1's per-thread load order
@@ -640,7 +648,7 @@ __global__ void __launch_bounds__(256)
 cdd_split_combine(const __grid_constant__ SplitArgs A)
 {
     constexpr int M = kSplitM, N = S * M;
-    const int L = N - A.overlap, half = A.overlap / 2;
+    const int L = N - A.overlap, head = A.overlap - A.lag;
     const float inv_n = 1.0f / (float)N;  // exact (power of two)
     const size_t total = (size_t)A.ndms * A.nitems * M;
     for(size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
@@ -663,8 +671,8 @@ cdd_split_combine(const __grid_constant__ SplitArgs A)
 #pragma unroll
         for(int n1 = 0; n1 < S; ++n1) {
             const int i = n2 + n1 * M;
-            const int m = start + i - half;
-            if(i >= half && i < half + L && m < A.nsamples) {
+            const int m = start + i - head;
+            if(i >= head && i < head + L && m < A.nsamples) {
                 const float fr = z[n1].x * inv_n, fi = z[n1].y * inv_n;
                 o_re[m] = (uint8_t)__float2int_rn(fr);
                 o_im[m] = (uint8_t)__float2int_rn(fi);
@@ -898,7 +906,7 @@ size_t sw_cdd_workspace_bytes(int nchans, int npol, int nant, int nsamples, int 
 }
 
 int sw_coherent_dedisperse_ws(const void* d_fpact_in, size_t row_stride, int nchans, int npol,
-                              int nant, int nsamples, int fft_len, int overlap,
+                              int nant, int nsamples, int fft_len, int overlap, int lag,
                               const void* d_setup, int ndms, void* const* h_d_out,
                               size_t out_row_stride, void* d_workspace,
                               size_t workspace_bytes, float* d_debug_f32,
@@ -909,8 +917,10 @@ int sw_coherent_dedisperse_ws(const void* d_fpact_in, size_t row_stride, int nch
                "coherent dedispersion: fft_len must be a power of two in [256, 65536]");
     SW_REQUIRE(d_fpact_in && d_setup && h_d_out, "coherent dedispersion: null pointer");
     SW_REQUIRE(ndms > 0 && ndms <= kMaxDms, "coherent dedispersion: 1..%d DMs", kMaxDms);
-    SW_REQUIRE(overlap >= 0 && overlap % 2 == 0 && overlap < fft_len,
-               "coherent dedispersion: overlap must be even and smaller than the FFT");
+    SW_REQUIRE(overlap >= 0 && overlap < fft_len,
+               "coherent dedispersion: overlap must be smaller than the FFT");
+    SW_REQUIRE(lag >= 0 && lag <= overlap,
+               "coherent dedispersion: the lag (%d) must lie in [0, overlap = %d]", lag, overlap);
     SW_REQUIRE(nsamples > 0 && (size_t)overlap + nsamples <= row_stride,
                "coherent dedispersion: input rows must hold history + gulp");
     SW_REQUIRE((size_t)nsamples <= out_row_stride, "coherent dedispersion: output rows too short");
@@ -933,6 +943,7 @@ int sw_coherent_dedisperse_ws(const void* d_fpact_in, size_t row_stride, int nch
         a.nstreams = nstreams;
         a.nsamples = nsamples;
         a.overlap = overlap;
+        a.lag = lag;
         a.nseg = nseg;
         a.ndms = ndms;
         a.npa = npol * nant;
@@ -961,6 +972,7 @@ int sw_coherent_dedisperse_ws(const void* d_fpact_in, size_t row_stride, int nch
     a.nstreams   = nstreams;
     a.nsamples   = nsamples;
     a.overlap    = overlap;
+    a.lag        = lag;
     a.nseg       = nseg;
     a.ndms       = ndms;
     a.tw         = tw;
@@ -983,7 +995,7 @@ int sw_coherent_dedisperse_ws(const void* d_fpact_in, size_t row_stride, int nch
 
 int sw_coherent_dedisperse(const void* d_fpact_in, size_t row_stride,
                            int nchans, int npol, int nant, int nsamples,
-                           int fft_len, int overlap, const void* d_setup,
+                           int fft_len, int overlap, int lag, const void* d_setup,
                            int ndms, void* const* h_d_out,
                            size_t out_row_stride, sw_stream_t stream)
 {
@@ -991,7 +1003,7 @@ int sw_coherent_dedisperse(const void* d_fpact_in, size_t row_stride,
                "coherent dedispersion: fft_len %d > %d needs sw_coherent_dedisperse_ws", fft_len,
                kSplitM);
     return sw_coherent_dedisperse_ws(d_fpact_in, row_stride, nchans, npol, nant, nsamples,
-                                     fft_len, overlap, d_setup, ndms, h_d_out, out_row_stride,
+                                     fft_len, overlap, lag, d_setup, ndms, h_d_out, out_row_stride,
                                      nullptr, 0, nullptr, stream);
 }
 

@@ -242,8 +242,10 @@ int launch_incoherent_beamform(const void* d_fpact, size_t row_stride,
     SW_REQUIRE(tscrunch > 0 && nsamples % tscrunch == 0,
                "sw_incoherent_beamform: nsamples must be a multiple of tscrunch");
     SW_REQUIRE(stokes >= 0 && stokes <= 4, "sw_incoherent_beamform: bad Stokes mode");
-    SW_REQUIRE(tscrunch % 4 != 0 || (row_stride % 4 == 0 && sample_offset % 4 == 0),
-               "sw_incoherent_beamform: stride/offset must be multiples of 4");
+    SW_REQUIRE(tscrunch % 4 != 0 || (row_stride % 4 == 0 && sample_offset % 4 == 0 &&
+                                     (reinterpret_cast<uintptr_t>(d_fpact) & 3) == 0),
+               "sw_incoherent_beamform: with tscrunch a multiple of 4 the voltage pointer, "
+               "row stride and sample offset must be multiples of 4 bytes");
     SW_REQUIRE(nchans > 0 && nchans <= 65535, "sw_incoherent_beamform: bad channel count");
     IbArgs args{static_cast<const uint8_t*>(d_fpact), row_stride, sample_offset,
                 nchans, nsamples, nant, tscrunch, nbeamsets, stokes, d_scale,

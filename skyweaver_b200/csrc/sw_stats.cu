@@ -192,7 +192,8 @@ namespace {
 
 // Device address of g_stats_noalloc_sums on the current device.  The host
 // symbol is only a stand-in, so the address is looked up once per device
-// (with that device current) and cached.
+// (with that device current) and cached for the process; cudaDeviceReset
+// would make the cached address stale, which the header documents.
 int noalloc_sums(long long** out)
 {
     static std::mutex mu;

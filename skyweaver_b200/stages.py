@@ -205,12 +205,30 @@ def dm_delay(f_ref, f, dm):
     return DM_CONST * (1 / (f_ref * f_ref) - 1 / (f * f)) * dm
 
 
+def cdd_plan(centre_frequency, bandwidth, nchans, dms, fft_len=0, lag=0):
+    """sw_cdd_plan (host only): the pipeline's overlap-save plan
+    (fft_len, overlap, lag) for this band and DM set."""
+    d = (ctypes.c_float * len(dms))(*[float(x) for x in dms])
+    n, o, g = ctypes.c_int(int(fft_len)), ctypes.c_int(), ctypes.c_int()
+    call("sw_cdd_plan", ctypes.c_double(centre_frequency), ctypes.c_double(bandwidth), nchans,
+         d, len(dms), int(lag), ctypes.byref(n), ctypes.byref(o), ctypes.byref(g))
+    return n.value, o.value, g.value
+
+
 class CoherentDedisperser:
     """create_coherent_dedisperser_config + CoherentDedisperser::dedisperse for
-    all channels/antennas/pols and DMs of a gulp (overlap-save with history)."""
+    all channels/antennas/pols and DMs of a gulp (overlap-save with history).
 
-    def __init__(self, nchans, nant, fft_len, overlap, low_freq, bw, dms, device="cuda"):
+    Every window trims overlap - lag samples at its start and lag at its end,
+    and the output is delayed by lag samples; lag=None is the reference's
+    overlap / 2 at each end (CoherentDedisperser.cu:196-223)."""
+
+    def __init__(self, nchans, nant, fft_len, overlap, low_freq, bw, dms, device="cuda",
+                 lag=None):
         self.nchans, self.nant, self.fft_len, self.overlap = nchans, nant, fft_len, overlap
+        self.lag = overlap // 2 if lag is None else int(lag)
+        if not 0 <= self.lag <= overlap:
+            raise ValueError("lag must lie in [0, overlap]")
         self.dms = np.asarray(dms, np.float32)
         nbytes = lib().sw_cdd_setup_bytes(len(dms), nchans, fft_len)
         if nbytes == 0:
@@ -244,7 +262,7 @@ class CoherentDedisperser:
         dbg = (torch.empty((nd, F, P, A, nsamples, 2), dtype=torch.float32,
                            device=fpact_ext.device) if debug else None)
         call("sw_coherent_dedisperse_ws", _ptr(fpact_ext), stride, F, P, A, nsamples,
-             self.fft_len, self.overlap, _ptr(self.setup), nd, arr, outs[0].shape[-1],
+             self.fft_len, self.overlap, self.lag, _ptr(self.setup), nd, arr, outs[0].shape[-1],
              _ptr(ws), ws.numel() if ws is not None else 0, _ptr(dbg), _stream(stream))
         return (outs, dbg) if debug else outs
 
@@ -275,7 +293,8 @@ def autotune(nantennas, nbeams, nchans, nsamples, tscrunch, dms, centre_frequenc
     call("sw_autotune", nantennas, nbeams, nchans, nsamples, tscrunch, len(dms), d,
          ctypes.c_double(centre_frequency), ctypes.c_double(bandwidth), ctypes.byref(t),
          _stream(stream))
-    return {"fft_len": t.fft_len, "overlap": t.overlap, "cb_tiles_per_item": t.cb_tiles_per_item,
+    return {"fft_len": t.fft_len, "overlap": t.overlap, "lag": t.lag,
+            "cb_tiles_per_item": t.cb_tiles_per_item,
             "cdd_ms": t.cdd_ms, "cb_ms": t.cb_ms}
 
 
@@ -324,20 +343,21 @@ class IncoherentDedispersionPipeline:
 
 
 # ------------------------------------------------------------------ pipeline
-def describe(dims, sizes, centre_frequency, bandwidth, nchans, tscrunch, overlap, dm):
+def describe(dims, sizes, centre_frequency, bandwidth, nchans, tscrunch, lag, dm):
     """The metadata the reference's DescribedVector carries beside its data
     (DescribedVector.hpp:96-573) for one pipeline output: dimension order and
     extents, channel centre frequencies (PipelineConfig.cpp:188-203), tsamp =
     tscrunch x channel sample (CoherentBeamformer.cu:235), utc_offset = the
-    coherent dedisperser's filter delay tsamp * overlap / 2
-    (CoherentDedisperser.cu:82) and reference_dm = the coherent DM
+    coherent dedisperser's filter delay, i.e. the delay of its output: `lag`
+    channel samples (the reference's symmetric trim makes it tsamp * overlap / 2,
+    CoherentDedisperser.cu:82) and reference_dm = the coherent DM
     (CoherentDedisperser.cu:224)."""
     chbw = bandwidth / nchans
     bottom = centre_frequency - bandwidth / 2.0
     chan_tsamp = nchans / bandwidth
     return {"dims": dims, "extents": tuple(int(x) for x in sizes),
             "frequencies": [bottom + chbw / 2.0 + chbw * i for i in range(nchans)],
-            "tsamp": chan_tsamp * tscrunch, "utc_offset": chan_tsamp * overlap / 2.0,
+            "tsamp": chan_tsamp * tscrunch, "utc_offset": chan_tsamp * lag,
             "dms": [], "reference_dm": float(dm)}
 
 
@@ -348,7 +368,7 @@ class BeamformerPipeline:
                  tscrunch, centre_frequency, bandwidth, dms, beamset_weights,
                  beamset_mapping, stokes="I", ib_subtract=True, output_level=24.0,
                  fft_len=0, coherent_dedispersion=True, grouped=True, use_graph=True,
-                 autotune=False):
+                 autotune=False, cdd_lag=0):
         self._dms = (ctypes.c_float * len(dms))(*[float(d) for d in dms])
         bw = np.ascontiguousarray(beamset_weights, np.float32)
         mp = np.ascontiguousarray(beamset_mapping, np.int32)
@@ -359,7 +379,7 @@ class BeamformerPipeline:
             nantennas, input_nantennas, nchans, nbeams, gulp_samples, tscrunch,
             STOKES[stokes], int(ib_subtract), output_level, centre_frequency, bandwidth,
             len(dms), self._dms, fft_len, int(coherent_dedispersion), int(grouped),
-            int(use_graph), bw.shape[0], self._bw, self._mp, int(autotune))
+            int(use_graph), bw.shape[0], self._bw, self._mp, int(autotune), int(cdd_lag))
         h = ctypes.c_void_p()
         call("sw_pipeline_create", ctypes.byref(cfg), ctypes.byref(h))
         self.h = h
@@ -380,9 +400,9 @@ class BeamformerPipeline:
     def _describe(self, dm_idx, dims, sizes, tscrunch):
         if not 0 <= dm_idx < self.ndms:
             raise IndexError(f"DM index {dm_idx} out of range")
-        _, overlap = self.fft_plan()
+        lag = self.cdd_plan()[2]
         return describe(dims, sizes, self._centre, self._bandwidth, self.nchans, tscrunch,
-                        overlap, self._dm_list[dm_idx])
+                        lag, self._dm_list[dm_idx])
 
     def describe_cb(self, dm_idx: int) -> dict:
         """DescribedVector metadata of one DM's coherent beams (TFB): the
@@ -416,9 +436,16 @@ class BeamformerPipeline:
              _ptr(cb_out_pinned), _stream(stream))
 
     def fft_plan(self):
-        n, o = ctypes.c_int(), ctypes.c_int()
-        call("sw_pipeline_fft_len", self.h, ctypes.byref(n), ctypes.byref(o))
-        return n.value, o.value
+        """(fft_len, overlap) of the coherent dedisperser."""
+        return self.cdd_plan()[:2]
+
+    def cdd_plan(self):
+        """(fft_len, overlap, lag): every window trims overlap - lag samples at
+        its start and lag at its end; the dedispersed voltages are delayed by
+        lag samples."""
+        n, o, g = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        call("sw_pipeline_fft_len", self.h, ctypes.byref(n), ctypes.byref(o), ctypes.byref(g))
+        return n.value, o.value, g.value
 
     def cb_device(self, dm_idx: int):
         """The last gulp's coherent beams of one DM as a device tensor view
@@ -428,6 +455,18 @@ class BeamformerPipeline:
         T = self.gulp // self.tscrunch
         shape = (T, self.nchans, self.nbeams) + ((4,) if self.stokes == "IQUV" else ())
         return _device_view(pcb.value, int(np.prod(shape))).view(torch.int8).reshape(shape)
+
+    def voltages(self, dm_idx: int):
+        """A copy of the last gulp's voltages that fed the beamformers for one
+        DM, as FPACT int8 [F][P][A][re|im][gulp] (dedispersed and delayed by the
+        plan's lag, or as transposed without coherent dedispersion)."""
+        p, stride = ctypes.c_void_p(), ctypes.c_size_t()
+        call("sw_pipeline_voltages", self.h, dm_idx, ctypes.byref(p), ctypes.byref(stride))
+        torch.cuda.synchronize()
+        rows = self.nchans * 2 * self._nant * 2
+        v = _device_view(p.value, (rows - 1) * stride.value + self.gulp).view(torch.int8)
+        return v.as_strided((rows, self.gulp), (stride.value, 1)).cpu().numpy().reshape(
+            self.nchans, 2, self._nant, 2, self.gulp)
 
     def cb_bytes_per_dm(self):
         return lib().sw_pipeline_cb_bytes_per_dm(self.h)

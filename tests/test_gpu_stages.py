@@ -328,31 +328,39 @@ def test_coherent_dedispersion_golden_vector(cuda):
     assert np.abs(got0.astype(int) - inp[overlap // 2: overlap // 2 + 446].astype(int)).max() <= 1
 
 
-@pytest.mark.parametrize("fft_len,dms", [(2048, [0.0, 50.0, 150.0]), (4096, [0.0, 500.0]),
-                                         (8192, [150.0]), (1024, [30.0]),
-                                         (16384, [0.0, 500.0]), (32768, [150.0])])
-def test_coherent_dedispersion_overlap_save(cuda, oracle, fft_len, dms):
+@pytest.mark.parametrize("fft_len,dms,lag", [(2048, [0.0, 50.0, 150.0], None),
+                                             (4096, [0.0, 500.0], 128), (8192, [150.0], 128),
+                                             (8192, [0.0, 50.0, 500.0], None), (1024, [30.0], 64),
+                                             (16384, [0.0, 500.0], 128), (32768, [150.0], None)])
+def test_coherent_dedispersion_overlap_save(cuda, oracle, fft_len, dms, lag):
+    """Every window trims overlap - lag samples at its start and lag at its
+    end: lag None is the reference's overlap / 2 at each end, the others the
+    pipeline's one-sided plan.  Against the FP64 oracle at the same plan."""
     from skyweaver_b200 import stages, synthetic
-    g = synthetic.rng(fft_len)
+    g = synthetic.rng(fft_len + (lag or 0))
     F, A, T = 2, 4, 8192
     chbw = 856e6 / 1024                      # MeerKAT L-band 1024-channel mode
     bw = F * chbw
     low = 1284e6 - 32 * chbw                 # bottom of a 64-channel subband
     tsamp = 1.0 / chbw
     smear = stages.dm_delay(low, low + bw / F, max(dms)) / tsamp
-    overlap = int(math.ceil(smear)) + 1 & ~1
+    if lag is None:
+        overlap = int(math.ceil(smear)) + 1 & ~1
+    else:
+        overlap = (int(math.ceil(smear)) + 15 & ~15) + lag
     assert overlap < fft_len
     ext = np.clip(np.rint(g.normal(0, 12, size=(F, 2, A, 2, overlap + T))), -127, 127).astype(np.int8)
-    cdd = stages.CoherentDedisperser(F, A, fft_len, overlap, low, bw, dms)
+    cdd = stages.CoherentDedisperser(F, A, fft_len, overlap, low, bw, dms, lag=lag)
     outs = cdd.dedisperse(_dev(cuda, ext), T)
     for d, dm in enumerate(dms):
         chirps = oracle.chirp(F, fft_len, low, bw, dm)
         ftpa_ext = ext.transpose(0, 4, 1, 2, 3)                  # [F][O+T][P][A][2]
-        ref, f64 = oracle.cdd_ftpa(ftpa_ext, T, chirps, overlap, want_f64=True)
+        ref, f64 = oracle.cdd_ftpa(ftpa_ext, T, chirps, overlap, want_f64=True, lag=lag)
         got = _np(outs[d]).transpose(0, 4, 1, 2, 3)
         diff = np.abs(got.astype(int) - ref.astype(int))
         frac = (diff > 0).mean()
-        print(f"fft {fft_len} DM {dm}: {(diff > 0).sum()} of {diff.size} differ by one LSB")
+        print(f"fft {fft_len} lag {lag} DM {dm}: {(diff > 0).sum()} of {diff.size} differ "
+              f"by one LSB")
         assert diff.max() <= 1, (dm, diff.max())
         assert frac <= 1e-5, (dm, frac)                       # measured: at most 2 of 262144
 
