@@ -253,7 +253,8 @@ int sw_cdd_chirps(const float* h_dms, int ndms, int nchans, int fft_len,
  * the whole subband's DM delay and takes the gulp as the FFT length).  Each
  * window trims, at its start, the largest intra-channel DM smear (lowest
  * channel, largest DM) rounded up to 16 samples and, at its end, `*lag`
- * samples (lag_request rounded up to 16; 0 = 128): *overlap is their sum.
+ * samples (lag_request rounded up to 16; 0 = 128; none when every DM is 0,
+ * whose chirp is exactly 1): *overlap is their sum.
  * *fft_len > 0 on entry is kept if it exceeds the overlap; 0 picks one by a
  * cost model (on-chip sizes up to 8192 first).  SW_ERR_INVALID if none fits. */
 int sw_cdd_plan(double centre_frequency, double bandwidth, int nchans,

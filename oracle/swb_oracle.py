@@ -236,12 +236,13 @@ def cdd_plan(centre_frequency, bandwidth, nchans, dms, fft_len=0, lag=128):
     smear of the lowest channel at the largest DM.  The window therefore
     trims that smear (rounded up to 16) at its start and a margin `lag`
     (rounded up to 16) at its end, which holds the response's short
-    anti-causal part; the output is delayed by `lag` samples."""
+    anti-causal part; the output is delayed by `lag` samples.  With every DM
+    0 the response is a unit impulse and nothing is trimmed."""
     chbw = bandwidth / nchans
     f_low = float(np.float32(centre_frequency - bandwidth / 2.0))
     smear = 4.148806423e15 * (1.0 / f_low ** 2 - 1.0 / (f_low + chbw) ** 2) * max(dms)
     head = (int(np.ceil(smear * chbw)) + 15) // 16 * 16
-    lag = (int(lag) + 15) // 16 * 16
+    lag = (int(lag) + 15) // 16 * 16 if head else 0   # every DM 0: a unit impulse
     overlap = head + lag
     if not fft_len:
         best = None

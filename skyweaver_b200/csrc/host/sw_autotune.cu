@@ -81,8 +81,9 @@ extern "C" int sw_autotune(int nantennas, int nbeams, int nchans, int nsamples, 
     SW_REQUIRE(nchans > 0 && nbeams > 0 && nsamples > 0 && nsamples % 64 == 0 && tscrunch > 0,
                "sw_autotune: bad shape");
     // the pipeline's default overlap-save plan (sw_host.hpp)
-    const int lag     = cdd_round_lag(0);
-    const int overlap = cdd_head(centre_frequency, bandwidth, nchans, h_dms, ndms) + lag;
+    const int head    = cdd_head(centre_frequency, bandwidth, nchans, h_dms, ndms);
+    const int lag     = cdd_round_lag(0, head);
+    const int overlap = head + lag;
     const Key key{nantennas, nbeams, nchans, nsamples, tscrunch, ndms, overlap};
     {
         std::lock_guard<std::mutex> lk(g_mu);

@@ -13,8 +13,9 @@ constexpr double kDmConst = 4.148806423e15;  // dedispersion_utils.cuh:12-13
 // all of it lies at causal lags up to the intra-channel DM smear of the lowest
 // channel at the largest DM.  A window therefore trims that smear, rounded up
 // to a multiple of 16, at its start (`head`) and `lag` samples (default 128,
-// rounded up to 16) at its end, which hold the response's short anti-causal
-// part; overlap = head + lag and the output is delayed by lag samples.
+// rounded up to 16; none when every DM is 0) at its end, which hold the
+// response's short anti-causal part; overlap = head + lag and the output is
+// delayed by lag samples.
 // Multiples of 16 keep every window start 16-byte aligned.
 constexpr int kCddDefaultLag = 128;
 
@@ -32,7 +33,14 @@ inline int cdd_head(double centre_frequency, double bandwidth, int nchans, const
     return (ov + 15) / 16 * 16;
 }
 
-inline int cdd_round_lag(int lag) { return ((lag > 0 ? lag : kCddDefaultLag) + 15) / 16 * 16; }
+// The lag for a plan whose head trim is `head`: none when every DM is 0 (the
+// chirp is exactly 1, the response a unit impulse), else the request (0 for
+// the default) rounded up to 16.
+inline int cdd_round_lag(int lag, int head)
+{
+    if(head == 0) return 0;
+    return ((lag > 0 ? lag : kCddDefaultLag) + 15) / 16 * 16;
+}
 
 // FFT length by a cost model (log2 N operations per sample over the useful
 // fraction 1 - overlap / N), on-chip sizes (<= 8192) when one exceeds the

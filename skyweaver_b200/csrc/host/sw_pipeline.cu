@@ -5,9 +5,14 @@
 // serial per-channel dedispersion launches; here one gulp is
 //
 //   [epoch H2D] -> weights -> TAFTP->FPACT transpose -> statistics
-//   -> (gulp 0: scalings) -> coherent dedispersion of all channels for all
-//   DMs -> history copy -> incoherent beam per DM
-//   -> one persistent grouped tensor-core launch for all (DM x beamset)
+//   -> (gulp 0: scalings) -> coherent dedispersion of all channels for every
+//   non-zero DM -> incoherent beam per DM -> one persistent grouped
+//   tensor-core launch for all (DM x beamset) -> history copy
+//
+// A DM of exactly 0 has a chirp of exactly 1: its dedispersed voltages are
+// the input delayed by the plan's lag, which the beamformers read straight
+// from the transposed rows (at offset overlap - lag), so it costs no
+// transform and no copy.
 //
 // all on one stream, captured once as a CUDA graph per input/output buffer
 // pair.  process_host double-buffers the pinned-host input and the outputs
@@ -74,6 +79,9 @@ struct sw_pipeline {
     int lag = 0;                   // of it, trimmed at each window's end
     int cb_tpi = 0;                // CB work-item size (0: kernel default)
     size_t ext_stride = 0, ext_off = 0, dd_stride = 0;
+    size_t v_off = 0;           // first sample of the beamformers' voltages in a row
+    std::vector<int> dd_of;     // per DM: index into dd (-1: DM 0, read from ext)
+    std::vector<float> cdd_dms; // the non-zero DMs, in order
     size_t nrows = 0;  // F * P * A * 2
 
     DevBuf taftp[2];
@@ -148,8 +156,9 @@ int sw_pipeline::init(const sw_pipeline_config& c)
     // DM smear (lowest channel, largest DM) at its start and `lag` samples at
     // its end; overlap = both, multiples of 16.
     if(c.enable_coherent_dedispersion) {
-        lag     = swb::cdd_round_lag(c.cdd_lag);
-        overlap = swb::cdd_head(c.centre_frequency, c.bandwidth, F, dms.data(), ndm) + lag;
+        const int head = swb::cdd_head(c.centre_frequency, c.bandwidth, F, dms.data(), ndm);
+        lag     = swb::cdd_round_lag(c.cdd_lag, head);
+        overlap = head + lag;
         if(c.fft_len > 0) {
             fft_len = c.fft_len;
         } else if(c.autotune) {
@@ -172,7 +181,16 @@ int sw_pipeline::init(const sw_pipeline_config& c)
     }
     ext_off    = (size_t)overlap;
     ext_stride = (size_t)overlap + T;
-    dd_stride  = (size_t)T;
+    // dedispersed rows share the transposed rows' geometry so that every DM's
+    // voltages start at the same offset: overlap - lag = the delayed gulp
+    dd_stride  = ext_stride;
+    v_off      = (size_t)(overlap - lag);
+    dd_of.assign(ndm, -1);
+    for(int d = 0; c.enable_coherent_dedispersion && d < ndm; ++d)
+        if(dms[d] != 0.0f) {
+            dd_of[d] = (int)cdd_dms.size();
+            cdd_dms.push_back(dms[d]);
+        }
     nrows      = (size_t)F * 2 * A * 2;
 
     SW_CUDA_CHECK(cudaStreamCreateWithFlags(&compute, cudaStreamNonBlocking));
@@ -191,19 +209,20 @@ int sw_pipeline::init(const sw_pipeline_config& c)
     SW_TRY(taftp[1].alloc(taftp_bytes));
     SW_TRY(ext.alloc(nrows * ext_stride));
     SW_CUDA_CHECK(cudaMemset(ext.p, 0, ext.n));  // zero history for gulp 0
-    if(c.enable_coherent_dedispersion) {
-        dd.resize(ndm);
-        for(int d = 0; d < ndm; ++d) SW_TRY(dd[d].alloc(nrows * dd_stride));
-        SW_TRY(d_setup.alloc(sw_cdd_setup_bytes(ndm, F, fft_len)));
+    const int ncdd = (int)cdd_dms.size();
+    if(c.enable_coherent_dedispersion && ncdd > 0) {
+        dd.resize(ncdd);
+        for(int k = 0; k < ncdd; ++k) SW_TRY(dd[k].alloc(nrows * dd_stride));
+        SW_TRY(d_setup.alloc(sw_cdd_setup_bytes(ncdd, F, fft_len)));
         // long FFTs (> 8192) pass their sub-transform spectra through a
         // workspace: at most 4 GiB, processed in chunks of segments
-        const size_t ws = sw_cdd_workspace_bytes(F, 2, A, T, fft_len, overlap, ndm);
+        const size_t ws = sw_cdd_workspace_bytes(F, 2, A, T, fft_len, overlap, ncdd);
         if(ws) {
-            const size_t per_seg = (size_t)ndm * fft_len * 8;
+            const size_t per_seg = (size_t)ncdd * fft_len * 8;
             SW_TRY(cdd_ws.alloc(std::max(per_seg, std::min(ws, (size_t)4 << 30) / per_seg * per_seg)));
         }
         const double low = (double)(float)(c.centre_frequency - c.bandwidth / 2.0f);
-        SW_TRY(sw_cdd_chirps(dms.data(), ndm, F, fft_len, low, c.bandwidth, d_setup.p,
+        SW_TRY(sw_cdd_chirps(cdd_dms.data(), ncdd, F, fft_len, low, c.bandwidth, d_setup.p,
                              (sw_stream_t)compute));
     }
     SW_TRY(stats.alloc((size_t)F * 2 * A * 4 * sizeof(float)));
@@ -258,21 +277,17 @@ int sw_pipeline::enqueue_chain(const void* d_in, int parity, bool first)
                                   cfg.output_level, cb_off.as<float>(), cb_scl.as<float>(),
                                   ib_off.as<float>(), ib_scl.as<float>(), ss));
     }
+    // every DM's voltages: rows of ext_stride samples from offset v_off
     std::vector<const void*> volt(ndm);
-    size_t vstride = ext_stride, voff = ext_off;
-    if(cfg.enable_coherent_dedispersion) {
-        std::vector<void*> outs(ndm);
-        for(int d = 0; d < ndm; ++d) outs[d] = dd[d].p;
+    const size_t vstride = ext_stride, voff = v_off;
+    if(!cdd_dms.empty()) {
+        std::vector<void*> outs(cdd_dms.size());
+        for(size_t k = 0; k < outs.size(); ++k) outs[k] = dd[k].as<uint8_t>() + v_off;
         SW_TRY(sw_coherent_dedisperse_ws(ext.p, ext_stride, F, 2, A, T, fft_len, overlap, lag,
-                                         d_setup.p, ndm, outs.data(), dd_stride, cdd_ws.p,
-                                         cdd_ws.n, nullptr, ss));
-        SW_TRY(sw_fpact_keep_history(ext.p, nrows, ext_stride, (size_t)overlap, ss));
-        for(int d = 0; d < ndm; ++d) volt[d] = dd[d].p;
-        vstride = dd_stride;
-        voff = 0;
-    } else {
-        for(int d = 0; d < ndm; ++d) volt[d] = ext.p;
+                                         d_setup.p, (int)outs.size(), outs.data(), dd_stride,
+                                         cdd_ws.p, cdd_ws.n, nullptr, ss));
     }
+    for(int d = 0; d < ndm; ++d) volt[d] = dd_of[d] < 0 ? ext.p : dd[dd_of[d]].p;
     for(int d = 0; d < ndm; ++d) {
         SW_TRY(swb::launch_incoherent_beamform(volt[d], vstride, voff, F, T, A, ts,
                                                ib_scl.as<float>(), ib_off.as<float>(),
@@ -315,6 +330,9 @@ int sw_pipeline::enqueue_chain(const void* d_in, int parity, bool first)
             SW_TRY(sw_coherent_beamform(&shape, &pr, d_wgemm.p, cb_scl.as<float>(),
                                         cb_off.as<float>(), d_map.as<int>(), nullptr, ss));
     }
+    // overlap-save history for the next gulp, once every reader of this
+    // gulp's rows (dedisperser, and the beamformers for a DM of 0) is done
+    if(overlap > 0) SW_TRY(sw_fpact_keep_history(ext.p, nrows, ext_stride, (size_t)overlap, ss));
     return SW_OK;
 }
 
@@ -361,8 +379,9 @@ int sw_cdd_plan(double centre_frequency, double bandwidth, int nchans, const flo
 {
     SW_REQUIRE(h_dms && ndms > 0 && nchans > 0 && bandwidth > 0.0 && fft_len && overlap && lag,
                "sw_cdd_plan: bad arguments");
-    const int lg = cdd_round_lag(lag_request);
-    const int ov = cdd_head(centre_frequency, bandwidth, nchans, h_dms, ndms) + lg;
+    const int head = cdd_head(centre_frequency, bandwidth, nchans, h_dms, ndms);
+    const int lg   = cdd_round_lag(lag_request, head);
+    const int ov   = head + lg;
     int n = *fft_len > 0 ? *fft_len : cdd_model_fft_len(ov);
     SW_REQUIRE(n > ov && n >= 256 && n <= 65536 && (n & (n - 1)) == 0,
                "coherent dedispersion: no power-of-two FFT length in [256, 65536] exceeds the "
@@ -469,13 +488,9 @@ int sw_pipeline_voltages(sw_pipeline* p, int dm_idx, const int8_t** d_fpact, siz
 {
     SW_REQUIRE(p && dm_idx >= 0 && dm_idx < p->ndm && d_fpact && row_stride,
                "sw_pipeline_voltages: bad arguments");
-    if(p->cfg.enable_coherent_dedispersion) {
-        *d_fpact    = p->dd[dm_idx].as<int8_t>();
-        *row_stride = p->dd_stride;
-    } else {
-        *d_fpact    = p->ext.as<int8_t>() + p->ext_off;
-        *row_stride = p->ext_stride;
-    }
+    const int k = p->dd_of[dm_idx];
+    *d_fpact    = (k < 0 ? p->ext.as<int8_t>() : p->dd[k].as<int8_t>()) + p->v_off;
+    *row_stride = p->ext_stride;
     return SW_OK;
 }
 

