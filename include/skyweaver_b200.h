@@ -105,6 +105,12 @@ int sw_fpact_to_ftpa(const void* d_fpact, void* d_ftpa, int nchans,
  * BufferedDispenser::hoard, cpp/skyweaver/src/BufferedDispenser.cu:29-66). */
 int sw_fpact_keep_history(void* d_fpact, size_t nrows, size_t row_stride,
                           size_t history, sw_stream_t stream);
+/* The same history copy between two row sets: the last `history` samples of
+ * every row of d_prev to the front of the same row of d_next (the pipeline
+ * alternates two row sets, so a gulp's rows stay intact while the next gulp
+ * is transposed). */
+int sw_fpact_copy_history(const void* d_prev, void* d_next, size_t nrows,
+                          size_t row_stride, size_t history, sw_stream_t stream);
 
 /* ------------------------------------------------------------------ */
 /* StatisticsCalculator                                                 */
@@ -480,10 +486,25 @@ int sw_pipeline_process_device(sw_pipeline* p, const void* d_taftp,
 int sw_pipeline_process_host(sw_pipeline* p, const void* h_taftp,
                              double epoch, void* h_cb_out,
                              sw_stream_t stream);
-/* Device pointers to the last gulp's outputs. */
+/* Device pointers to the last gulp's outputs (ordered on the stream given to
+ * the process call; no host wait).  The outputs alternate between two buffer
+ * sets, so they stay valid until the next-but-one gulp is processed. */
 int sw_pipeline_outputs(sw_pipeline* p, int dm_idx, const int8_t** d_cb_tfb,
                         const float** d_ib_raw, const int8_t** d_ib_btf,
                         const float** d_stats);
+/* Gulps processed so far. */
+long sw_pipeline_gulp_count(const sw_pipeline* p);
+/* The outputs of gulp number `gulp` (one of the last two processed), after a
+ * host wait for that gulp's chain to finish on the device: a caller can hand
+ * gulp g-1's beams to its handlers while gulp g computes (the reference
+ * pipeline synchronises every gulp instead, detail/BeamformerPipeline.cu:
+ * 265-301). */
+int sw_pipeline_gulp_outputs(sw_pipeline* p, long gulp, int dm_idx,
+                             const int8_t** d_cb_tfb, const float** d_ib_raw,
+                             const int8_t** d_ib_btf, const float** d_stats);
+/* Host wait until the last gulp's pinned input has been copied to the device,
+ * after which the caller may reuse that host buffer. */
+int sw_pipeline_wait_input(sw_pipeline* p);
 /* The last gulp's voltages that fed the beamformers for one DM: the
  * dedispersed FPACT rows (nsamples of the gulp from the row start, delayed
  * by the plan's lag), or the transposed gulp without coherent dedispersion

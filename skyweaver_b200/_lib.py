@@ -127,6 +127,11 @@ _SIGS = {
     "sw_pipeline_cb_bytes_per_dm": (c_size_t, [c_void_p]),
     "sw_cdd_plan": (c_int, [c_double, c_double, c_int, c_float_p, c_int, c_int,
                             ctypes.POINTER(c_int), ctypes.POINTER(c_int), ctypes.POINTER(c_int)]),
+    "sw_pipeline_gulp_count": (ctypes.c_long, [c_void_p]),
+    "sw_pipeline_gulp_outputs": (c_int, [c_void_p, ctypes.c_long, c_int,
+                                         ctypes.POINTER(c_void_p), ctypes.POINTER(c_void_p),
+                                         ctypes.POINTER(c_void_p), ctypes.POINTER(c_void_p)]),
+    "sw_pipeline_wait_input": (c_int, [c_void_p]),
     "sw_pipeline_voltages": (c_int, [c_void_p, c_int, ctypes.POINTER(c_void_p),
                                      ctypes.POINTER(c_size_t)]),
     "sw_pipeline_fft_len": (c_int, [c_void_p, ctypes.POINTER(c_int), ctypes.POINTER(c_int),

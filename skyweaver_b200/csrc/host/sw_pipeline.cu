@@ -4,10 +4,10 @@
 // reference runs ~10 synchronising stage calls per DM per gulp and 64
 // serial per-channel dedispersion launches; here one gulp is
 //
-//   [epoch H2D] -> weights -> TAFTP->FPACT transpose -> statistics
-//   -> (gulp 0: scalings) -> coherent dedispersion of all channels for every
-//   non-zero DM -> incoherent beam per DM -> one persistent grouped
-//   tensor-core launch for all (DM x beamset) -> history copy
+//   [epoch H2D] -> weights -> history copy -> TAFTP->FPACT transpose
+//   -> statistics -> (gulp 0: scalings) -> coherent dedispersion of all
+//   channels for every non-zero DM -> incoherent beam per DM -> one
+//   persistent grouped tensor-core launch for all (DM x beamset)
 //
 // A DM of exactly 0 has a chirp of exactly 1: its dedispersed voltages are
 // the input delayed by the plan's lag, which the beamformers read straight
@@ -85,9 +85,9 @@ struct sw_pipeline {
     size_t nrows = 0;  // F * P * A * 2
 
     DevBuf taftp[2];
-    DevBuf ext;
+    DevBuf ext[2];  // transposed rows [overlap history | gulp] per output parity
     std::vector<DevBuf> dd;
-    DevBuf stats, stats_scratch;
+    DevBuf stats[2], stats_scratch;  // statistics per output parity
     DevBuf ib_order;  // channels by descending power, for the incoherent beam
     DevBuf cb_off, cb_scl, ib_off, ib_scl;
     DevBuf d_bw, d_map, d_delays, d_freqs, d_wgemm, d_setup, cdd_ws;
@@ -207,8 +207,10 @@ int sw_pipeline::init(const sw_pipeline_config& c)
     const size_t taftp_bytes = (size_t)nheaps * c.input_nantennas * F * 256 * 2 * 2;
     SW_TRY(taftp[0].alloc(taftp_bytes));
     SW_TRY(taftp[1].alloc(taftp_bytes));
-    SW_TRY(ext.alloc(nrows * ext_stride));
-    SW_CUDA_CHECK(cudaMemset(ext.p, 0, ext.n));  // zero history for gulp 0
+    for(DevBuf& b : ext) {
+        SW_TRY(b.alloc(nrows * ext_stride));
+        SW_CUDA_CHECK(cudaMemset(b.p, 0, b.n));  // zero history for gulp 0
+    }
     const int ncdd = (int)cdd_dms.size();
     if(c.enable_coherent_dedispersion && ncdd > 0) {
         dd.resize(ncdd);
@@ -225,7 +227,7 @@ int sw_pipeline::init(const sw_pipeline_config& c)
         SW_TRY(sw_cdd_chirps(cdd_dms.data(), ncdd, F, fft_len, low, c.bandwidth, d_setup.p,
                              (sw_stream_t)compute));
     }
-    SW_TRY(stats.alloc((size_t)F * 2 * A * 4 * sizeof(float)));
+    for(DevBuf& b : stats) SW_TRY(b.alloc((size_t)F * 2 * A * 4 * sizeof(float)));
     SW_TRY(stats_scratch.alloc(sw_statistics_scratch_bytes(F, 2, A)));
     if(F <= swb::kIbOrderMaxChans) SW_TRY(ib_order.alloc((size_t)F * sizeof(int)));
     for(DevBuf* b : {&cb_off, &cb_scl, &ib_off, &ib_scl}) SW_TRY(b->alloc((size_t)S * F * sizeof(float)));
@@ -263,17 +265,23 @@ int sw_pipeline::enqueue_chain(const void* d_in, int parity, bool first)
                                   cudaMemcpyHostToDevice, s));
     SW_TRY(swb::launch_weights(d_delays.as<float>(), d_freqs.as<double>(), A, B, F, 0.0, 0.0,
                                d_ep, nullptr, d_wgemm.p, s));
-    SW_TRY(sw_transpose_fpact(d_in, ext.p, nheaps, cfg.input_nantennas, A, F, ext_stride,
+    // overlap-save history: the previous gulp's last `overlap` samples
+    void* rows = ext[parity].p;
+    if(overlap > 0)
+        SW_TRY(sw_fpact_copy_history(ext[parity ^ 1].p, rows, nrows, ext_stride,
+                                     (size_t)overlap, ss));
+    SW_TRY(sw_transpose_fpact(d_in, rows, nheaps, cfg.input_nantennas, A, F, ext_stride,
                               ext_off, ss));
-    SW_TRY(sw_statistics(ext.p, ext_stride, ext_off, F, 2, A, T, stats_scratch.p,
-                         stats.as<float>(), ss));
+    SW_TRY(sw_statistics(rows, ext_stride, ext_off, F, 2, A, T, stats_scratch.p,
+                         stats[parity].as<float>(), ss));
     const int* chan_order = nullptr;
     if(ib_order.p) {
-        SW_TRY(swb::launch_ib_channel_order(stats.as<float>(), F, 2, A, ib_order.as<int>(), s));
+        SW_TRY(swb::launch_ib_channel_order(stats[parity].as<float>(), F, 2, A,
+                                            ib_order.as<int>(), s));
         chan_order = ib_order.as<int>();
     }
     if(first) {
-        SW_TRY(sw_update_scalings(stats.as<float>(), d_bw.as<float>(), S, F, 2, A, ts, ts,
+        SW_TRY(sw_update_scalings(stats[parity].as<float>(), d_bw.as<float>(), S, F, 2, A, ts, ts,
                                   cfg.output_level, cb_off.as<float>(), cb_scl.as<float>(),
                                   ib_off.as<float>(), ib_scl.as<float>(), ss));
     }
@@ -283,11 +291,11 @@ int sw_pipeline::enqueue_chain(const void* d_in, int parity, bool first)
     if(!cdd_dms.empty()) {
         std::vector<void*> outs(cdd_dms.size());
         for(size_t k = 0; k < outs.size(); ++k) outs[k] = dd[k].as<uint8_t>() + v_off;
-        SW_TRY(sw_coherent_dedisperse_ws(ext.p, ext_stride, F, 2, A, T, fft_len, overlap, lag,
+        SW_TRY(sw_coherent_dedisperse_ws(rows, ext_stride, F, 2, A, T, fft_len, overlap, lag,
                                          d_setup.p, (int)outs.size(), outs.data(), dd_stride,
                                          cdd_ws.p, cdd_ws.n, nullptr, ss));
     }
-    for(int d = 0; d < ndm; ++d) volt[d] = dd_of[d] < 0 ? ext.p : dd[dd_of[d]].p;
+    for(int d = 0; d < ndm; ++d) volt[d] = dd_of[d] < 0 ? rows : dd[dd_of[d]].p;
     for(int d = 0; d < ndm; ++d) {
         SW_TRY(swb::launch_incoherent_beamform(volt[d], vstride, voff, F, T, A, ts,
                                                ib_scl.as<float>(), ib_off.as<float>(),
@@ -330,9 +338,6 @@ int sw_pipeline::enqueue_chain(const void* d_in, int parity, bool first)
             SW_TRY(sw_coherent_beamform(&shape, &pr, d_wgemm.p, cb_scl.as<float>(),
                                         cb_off.as<float>(), d_map.as<int>(), nullptr, ss));
     }
-    // overlap-save history for the next gulp, once every reader of this
-    // gulp's rows (dedisperser, and the beamformers for a DM of 0) is done
-    if(overlap > 0) SW_TRY(sw_fpact_keep_history(ext.p, nrows, ext_stride, (size_t)overlap, ss));
     return SW_OK;
 }
 
@@ -432,14 +437,15 @@ int sw_pipeline_process_device(sw_pipeline* p, const void* d_taftp, double epoch
 {
     SW_REQUIRE(p && d_taftp, "sw_pipeline_process_device: null argument");
     cudaStream_t s = as_cuda(stream);
+    const int par = (int)(p->gulp & 1);  // outputs alternate between two buffers
     // order after the caller's stream, run, and make the caller's stream wait
-    SW_CUDA_CHECK(cudaEventRecord(p->h2d_done[0], s));
-    SW_CUDA_CHECK(cudaStreamWaitEvent(p->compute, p->h2d_done[0], 0));
-    SW_CUDA_CHECK(cudaStreamWaitEvent(p->compute, p->d2h_done[0], 0));
-    int rc = p->run(d_taftp, 0, epoch);
+    SW_CUDA_CHECK(cudaEventRecord(p->h2d_done[par], s));
+    SW_CUDA_CHECK(cudaStreamWaitEvent(p->compute, p->h2d_done[par], 0));
+    SW_CUDA_CHECK(cudaStreamWaitEvent(p->compute, p->d2h_done[par], 0));
+    int rc = p->run(d_taftp, par, epoch);
     if(rc != SW_OK) return rc;
-    SW_CUDA_CHECK(cudaEventRecord(p->comp_done[0], p->compute));
-    SW_CUDA_CHECK(cudaStreamWaitEvent(s, p->comp_done[0], 0));
+    SW_CUDA_CHECK(cudaEventRecord(p->comp_done[par], p->compute));
+    SW_CUDA_CHECK(cudaStreamWaitEvent(s, p->comp_done[par], 0));
     ++p->gulp;
     return SW_OK;
 }
@@ -480,7 +486,7 @@ int sw_pipeline_outputs(sw_pipeline* p, int dm_idx, const int8_t** d_cb_tfb,
     if(d_cb_tfb) *d_cb_tfb = p->cb[par][dm_idx].as<int8_t>();
     if(d_ib_raw) *d_ib_raw = p->ib_raw[par][dm_idx].as<float>();
     if(d_ib_btf) *d_ib_btf = p->ib_i8[par][dm_idx].as<int8_t>();
-    if(d_stats) *d_stats = p->stats.as<float>();
+    if(d_stats) *d_stats = p->stats[par].as<float>();
     return SW_OK;
 }
 
@@ -489,8 +495,34 @@ int sw_pipeline_voltages(sw_pipeline* p, int dm_idx, const int8_t** d_fpact, siz
     SW_REQUIRE(p && dm_idx >= 0 && dm_idx < p->ndm && d_fpact && row_stride,
                "sw_pipeline_voltages: bad arguments");
     const int k = p->dd_of[dm_idx];
-    *d_fpact    = (k < 0 ? p->ext.as<int8_t>() : p->dd[k].as<int8_t>()) + p->v_off;
+    *d_fpact    = (k < 0 ? p->ext[p->last_par].as<int8_t>() : p->dd[k].as<int8_t>()) + p->v_off;
     *row_stride = p->ext_stride;
+    return SW_OK;
+}
+
+long sw_pipeline_gulp_count(const sw_pipeline* p) { return p ? p->gulp : 0; }
+
+int sw_pipeline_gulp_outputs(sw_pipeline* p, long gulp, int dm_idx, const int8_t** d_cb_tfb,
+                             const float** d_ib_raw, const int8_t** d_ib_btf,
+                             const float** d_stats)
+{
+    SW_REQUIRE(p && dm_idx >= 0 && dm_idx < p->ndm, "sw_pipeline_gulp_outputs: bad arguments");
+    SW_REQUIRE(gulp >= 0 && gulp < p->gulp && gulp >= p->gulp - 2,
+               "sw_pipeline_gulp_outputs: gulp %ld is not one of the last two processed "
+               "(%ld processed)", gulp, p->gulp);
+    const int par = (int)(gulp & 1);
+    SW_CUDA_CHECK(cudaEventSynchronize(p->comp_done[par]));
+    if(d_cb_tfb) *d_cb_tfb = p->cb[par][dm_idx].as<int8_t>();
+    if(d_ib_raw) *d_ib_raw = p->ib_raw[par][dm_idx].as<float>();
+    if(d_ib_btf) *d_ib_btf = p->ib_i8[par][dm_idx].as<int8_t>();
+    if(d_stats) *d_stats = p->stats[par].as<float>();
+    return SW_OK;
+}
+
+int sw_pipeline_wait_input(sw_pipeline* p)
+{
+    SW_REQUIRE(p, "sw_pipeline_wait_input: null pipeline");
+    if(p->gulp > 0) SW_CUDA_CHECK(cudaEventSynchronize(p->h2d_done[(p->gulp - 1) & 1]));
     return SW_OK;
 }
 

@@ -136,7 +136,9 @@ __global__ void ftpa_to_fpact_k(const int8_t* __restrict__ ftpa,
     }
 }
 
-__global__ void keep_history_k(uint4* __restrict__ fpact, size_t nrows,
+// the last history16 16-byte chunks of every row of `src` to the front of
+// the same row of `dst` (src == dst: in place)
+__global__ void keep_history_k(const uint4* src, uint4* dst, size_t nrows,
                                size_t row_stride16, size_t history16,
                                size_t nsamples16)
 {
@@ -144,8 +146,7 @@ __global__ void keep_history_k(uint4* __restrict__ fpact, size_t nrows,
     for(size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total;
         i += (size_t)gridDim.x * blockDim.x) {
         const size_t row = i / history16, k = i % history16;
-        uint4* r = fpact + row * row_stride16;
-        r[k] = r[nsamples16 + k];
+        dst[row * row_stride16 + k] = src[row * row_stride16 + nsamples16 + k];
     }
 }
 
@@ -252,8 +253,28 @@ int sw_fpact_keep_history(void* d_fpact, size_t nrows, size_t row_stride,
     const size_t nsamples = row_stride - history;
     const size_t work = nrows * (history / 16);
     keep_history_k<<<grid_for(work, 256), 256, 0, as_cuda(stream)>>>(
-        static_cast<uint4*>(d_fpact), nrows, row_stride / 16, history / 16,
-        nsamples / 16);
+        static_cast<const uint4*>(d_fpact), static_cast<uint4*>(d_fpact), nrows,
+        row_stride / 16, history / 16, nsamples / 16);
+    SW_LAUNCH_CHECK();
+    return SW_OK;
+}
+
+int sw_fpact_copy_history(const void* d_prev, void* d_next, size_t nrows, size_t row_stride,
+                          size_t history, sw_stream_t stream)
+{
+    SW_REQUIRE(d_prev && d_next, "sw_fpact_copy_history: null pointer");
+    SW_REQUIRE(row_stride % 16 == 0 && history % 16 == 0 &&
+                   (reinterpret_cast<uintptr_t>(d_prev) & 15) == 0 &&
+                   (reinterpret_cast<uintptr_t>(d_next) & 15) == 0,
+               "sw_fpact_copy_history: pointers, stride and history must be multiples of 16");
+    if(history == 0 || nrows == 0) return SW_OK;
+    SW_REQUIRE(row_stride >= 2 * history,
+               "sw_fpact_copy_history: rows must hold at least twice the history");
+    const size_t nsamples = row_stride - history;
+    const size_t work = nrows * (history / 16);
+    keep_history_k<<<grid_for(work, 256), 256, 0, as_cuda(stream)>>>(
+        static_cast<const uint4*>(d_prev), static_cast<uint4*>(d_next), nrows,
+        row_stride / 16, history / 16, nsamples / 16);
     SW_LAUNCH_CHECK();
     return SW_OK;
 }
