@@ -308,6 +308,21 @@ int sw_coherent_dedisperse_ws(const void* d_fpact_in, size_t row_stride,
                               size_t workspace_bytes, float* d_debug_f32,
                               sw_stream_t stream);
 
+/* Replaces CoherentDedisperser::dedisperse(tpa, ftpa, freq_idx, dm_idx)
+ * call by call (cpp/skyweaver/CoherentDedisperser.cuh:77-80): one channel,
+ * one DM of a setup that sw_cdd_chirps built for setup_nchans channels and
+ * setup_ndms DMs; input and output rows as for sw_coherent_dedisperse
+ * (npol x nant streams of the one channel).  fft_len > 8192 needs the
+ * workspace sw_cdd_workspace_bytes gives for one DM. */
+int sw_coherent_dedisperse_channel(const void* d_fpact_in, size_t row_stride,
+                                   int npol, int nant, int nsamples,
+                                   int fft_len, int overlap, int lag,
+                                   const void* d_setup, int setup_ndms,
+                                   int setup_nchans, int freq_idx, int dm_idx,
+                                   void* d_out, size_t out_row_stride,
+                                   void* d_workspace, size_t workspace_bytes,
+                                   sw_stream_t stream);
+
 /* ------------------------------------------------------------------ */
 /* IncoherentDedisperser                                                */
 /* ------------------------------------------------------------------ */
@@ -482,7 +497,9 @@ int sw_pipeline_set_delays(sw_pipeline* p, const float* h_delays,
 int sw_pipeline_process_device(sw_pipeline* p, const void* d_taftp,
                                double epoch, sw_stream_t stream);
 /* Run one gulp from pinned host memory: H2D copy, chain, and D2H of the
- * coherent-beam output of every DM into h_cb_out (may be NULL). */
+ * coherent-beam output of every DM into h_cb_out (may be NULL).  The chain
+ * is ordered after the work already queued on `stream`, and `stream` waits
+ * for the D2H. */
 int sw_pipeline_process_host(sw_pipeline* p, const void* h_taftp,
                              double epoch, void* h_cb_out,
                              sw_stream_t stream);

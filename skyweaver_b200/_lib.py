@@ -103,6 +103,10 @@ _SIGS = {
     "sw_coherent_dedisperse_ws": (c_int, [c_void_p, c_size_t, c_int, c_int, c_int, c_int, c_int,
                                           c_int, c_int, c_void_p, c_int, ctypes.POINTER(c_void_p),
                                           c_size_t, c_void_p, c_size_t, c_void_p, c_void_p]),
+    "sw_coherent_dedisperse_channel": (c_int, [c_void_p, c_size_t, c_int, c_int, c_int, c_int,
+                                               c_int, c_int, c_void_p, c_int, c_int, c_int,
+                                               c_int, c_void_p, c_size_t, c_void_p, c_size_t,
+                                               c_void_p]),
     "sw_idd_pipeline_create": (c_int, [c_int, c_int, c_int, ctypes.POINTER(c_int),
                                        ctypes.POINTER(c_void_p), ctypes.POINTER(c_int),
                                        c_float_p, ctypes.POINTER(c_int), c_void_p, c_void_p,

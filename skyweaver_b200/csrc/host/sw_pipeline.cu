@@ -98,7 +98,7 @@ struct sw_pipeline {
     bool have_delays = false;
 
     cudaStream_t compute = nullptr, h2d = nullptr, d2h = nullptr;
-    cudaEvent_t h2d_done[2]{}, comp_done[2]{}, d2h_done[2]{};
+    cudaEvent_t h2d_done[2]{}, comp_done[2]{}, d2h_done[2]{}, caller_ready[2]{};
     bool scalings_done = false;
     long gulp = 0;
     int last_par = 0;  // output parity of the last processed gulp
@@ -111,6 +111,7 @@ struct sw_pipeline {
             if(h2d_done[i]) cudaEventDestroy(h2d_done[i]);
             if(comp_done[i]) cudaEventDestroy(comp_done[i]);
             if(d2h_done[i]) cudaEventDestroy(d2h_done[i]);
+            if(caller_ready[i]) cudaEventDestroy(caller_ready[i]);
         }
         if(compute) cudaStreamDestroy(compute);
         if(h2d) cudaStreamDestroy(h2d);
@@ -200,6 +201,7 @@ int sw_pipeline::init(const sw_pipeline_config& c)
         SW_CUDA_CHECK(cudaEventCreateWithFlags(&h2d_done[i], cudaEventDisableTiming));
         SW_CUDA_CHECK(cudaEventCreateWithFlags(&comp_done[i], cudaEventDisableTiming));
         SW_CUDA_CHECK(cudaEventCreateWithFlags(&d2h_done[i], cudaEventDisableTiming));
+        SW_CUDA_CHECK(cudaEventCreateWithFlags(&caller_ready[i], cudaEventDisableTiming));
     }
     SW_CUDA_CHECK(cudaMallocHost(&h_epochs, 4 * sizeof(double)));
     memset(h_epochs, 0, 4 * sizeof(double));
@@ -455,6 +457,10 @@ int sw_pipeline_process_host(sw_pipeline* p, const void* h_taftp, double epoch, 
 {
     SW_REQUIRE(p && h_taftp, "sw_pipeline_process_host: null argument");
     const int par = (int)(p->gulp & 1);
+    // the chain runs after the work already on the caller's stream (e.g. a
+    // handler still reading the outputs this parity is about to overwrite)
+    SW_CUDA_CHECK(cudaEventRecord(p->caller_ready[par], as_cuda(stream)));
+    SW_CUDA_CHECK(cudaStreamWaitEvent(p->compute, p->caller_ready[par], 0));
     // H2D into this parity's input buffer once its previous gulp consumed it
     SW_CUDA_CHECK(cudaStreamWaitEvent(p->h2d, p->comp_done[par], 0));
     SW_CUDA_CHECK(cudaMemcpyAsync(p->taftp[par].p, h_taftp, p->taftp[par].n,

@@ -229,7 +229,8 @@ struct Args {
     int ndms;
     const c32* tw;     // twiddle tables
     const c32* chirp;  // [ndms][F][N] in per-thread load order (chirp_k)
-    const uint32_t* zero_dms;  // bit d: DM d is 0 (its chirp is exactly 1)
+    size_t chirp_dm_stride;    // complex entries between two DMs' tables
+    const uint32_t* zero_flags;  // [ndms]: non-zero if the DM is 0 (chirp exactly 1)
     int npa;           // P * A (streams per channel)
     uint8_t* out[kMaxDms];
     size_t out_stride;
@@ -384,7 +385,9 @@ cdd_kernel(const __grid_constant__ Args A)
     // (the FP32 round trip of int8 samples rounds back to them exactly), so
     // they are copied from the staged window instead of transformed.  The
     // debug instance transforms them to report the float round trip.
-    const uint32_t zero_dms = DBG ? 0u : *A.zero_dms;
+    uint32_t zero_dms = 0;
+    if constexpr(!DBG)
+        for(int d = 0; d < A.ndms && d < 32; ++d) zero_dms |= (A.zero_flags[d] ? 1u : 0u) << d;
     const bool copy16 = aligned && (head % 16) == 0 && (A.out_stride % 16) == 0;
     if(blockIdx.x < nitems) stage_input<N, NT>(stage, A, blockIdx.x, L, aligned);
     for(int item = blockIdx.x; item < nitems; item += gridDim.x) {
@@ -459,7 +462,7 @@ cdd_kernel(const __grid_constant__ Args A)
         for(int r = 0; r < 16; ++r) spec[r] = buf[pad(threadIdx.x * 16 + r)];
         dft16<false>(spec);
 
-        const size_t chirp_stride = (size_t)(A.nstreams / A.npa) * N;  // per DM
+        const size_t chirp_stride = A.chirp_dm_stride;  // complex entries per DM
         const float4* chp = reinterpret_cast<const float4*>(A.chirp + (size_t)f * N) + threadIdx.x;
         // the transformed DMs in order; chn holds the chirp of DM `d`
         int d = 0;
@@ -552,6 +555,7 @@ struct SplitArgs {
     const uint8_t* in;
     size_t row_stride;
     int nstreams, nsamples, overlap, lag, nseg, ndms, npa;
+    size_t chirp_dm_stride;  // complex entries between two DMs' tables
     int item0, nitems;  // work items [item0, item0 + nitems) of this chunk
     const c32* tw;      // M-point plan tables
     const c32* chirp;   // [ndms][F][S][M]: bin k1 + S k2 at k1's per-thread load order
@@ -634,7 +638,7 @@ cdd_split_kernel(const __grid_constant__ SplitArgs A)
 #pragma unroll
         for(int r = 0; r < 16; ++r) spec[r] = buf[pad(threadIdx.x * 16 + r)];
         dft16<false>(spec);
-        const size_t chirp_dm = (size_t)(A.nstreams / A.npa) * N;  // complex per DM
+        const size_t chirp_dm = A.chirp_dm_stride;  // complex per DM
         const float4* chp = reinterpret_cast<const float4*>(A.chirp + (size_t)f * N + (size_t)k1 * M) + threadIdx.x;
         __syncthreads();
         for(int d = 0; d < A.ndms; ++d) {
@@ -753,7 +757,10 @@ struct SetupArgs {
     double prefactor[kMaxDms];
 };
 
-__global__ void set_word_k(uint32_t* p, uint32_t v) { *p = v; }
+struct ZeroFlags {
+    uint32_t f[kMaxDms];
+};
+__global__ void set_flags_k(uint32_t* p, ZeroFlags z) { p[threadIdx.x] = z.f[threadIdx.x]; }
 
 __global__ void twiddle_k(c32* tw, int logn)
 {
@@ -882,6 +889,106 @@ int log2_exact(int n)
     return (1 << l) == n ? l : -1;
 }
 
+// Setup block: per-pass twiddles, a gap of kSetupGap complex entries whose
+// first words flag the DMs of exactly 0, the chirp tables [ndms][nchans][N]
+// and, for split transforms, the W_N^(n2 k1) table.
+constexpr int kSetupGap = 64;  // >= kMaxDms 32-bit flags
+
+// Dedisperse `nchans` channels (of a setup built for setup_nchans channels
+// and setup_ndms DMs, starting at channel chan0) for `ndms` DMs starting at
+// dm0 of the setup.
+int launch_cdd(const void* d_fpact_in, size_t row_stride, int nchans, int npol, int nant,
+               int nsamples, int fft_len, int overlap, int lag, const void* d_setup,
+               int setup_ndms, int setup_nchans, int chan0, int dm0, int ndms,
+               void* const* h_d_out, size_t out_row_stride, void* d_workspace,
+               size_t workspace_bytes, float* d_debug_f32, sw_stream_t stream)
+{
+    const int logn = log2_exact(fft_len);
+    SW_REQUIRE(logn >= 8 && logn <= 16,
+               "coherent dedispersion: fft_len must be a power of two in [256, 65536]");
+    SW_REQUIRE(d_fpact_in && d_setup && h_d_out, "coherent dedispersion: null pointer");
+    SW_REQUIRE(ndms > 0 && ndms <= kMaxDms, "coherent dedispersion: 1..%d DMs", kMaxDms);
+    SW_REQUIRE(overlap >= 0 && overlap < fft_len,
+               "coherent dedispersion: overlap must be smaller than the FFT");
+    SW_REQUIRE(lag >= 0 && lag <= overlap,
+               "coherent dedispersion: the lag (%d) must lie in [0, overlap = %d]", lag, overlap);
+    SW_REQUIRE(nsamples > 0 && (size_t)overlap + nsamples <= row_stride,
+               "coherent dedispersion: input rows must hold history + gulp");
+    SW_REQUIRE((size_t)nsamples <= out_row_stride, "coherent dedispersion: output rows too short");
+    SW_REQUIRE(nchans > 0 && npol > 0 && nant > 0, "coherent dedispersion: empty shape");
+    const int plog = logn > kSplitLog ? kSplitLog : logn;
+    const Plan P = make_plan(plog);
+    const c32* tw = static_cast<const c32*>(d_setup);
+    const c32* ch_all = tw + P.tw_total + kSetupGap;
+    const c32* ch = ch_all + ((size_t)dm0 * setup_nchans + chan0) * fft_len;
+    const uint32_t* zero_flags = reinterpret_cast<const uint32_t*>(tw + P.tw_total) + dm0;
+    const int nstreams = nchans * npol * nant;
+    const int nseg = cdiv(nsamples, fft_len - overlap);
+    cudaStream_t s = as_cuda(stream);
+    if(logn > kSplitLog) {
+        const size_t per_item = (size_t)ndms * fft_len * sizeof(c32);
+        SW_REQUIRE(d_workspace && workspace_bytes >= per_item,
+                   "coherent dedispersion: fft_len %d needs a workspace of at least %zu bytes "
+                   "(sw_cdd_workspace_bytes)", fft_len, per_item);
+        SplitArgs a{};
+        a.in = static_cast<const uint8_t*>(d_fpact_in);
+        a.row_stride = row_stride;
+        a.nstreams = nstreams;
+        a.nsamples = nsamples;
+        a.overlap = overlap;
+        a.lag = lag;
+        a.nseg = nseg;
+        a.ndms = ndms;
+        a.npa = npol * nant;
+        a.chirp_dm_stride = (size_t)setup_nchans * fft_len;
+        a.tw = tw;
+        a.chirp = ch;
+        a.tws = ch_all + (size_t)setup_ndms * setup_nchans * fft_len;
+        a.z = static_cast<c32*>(d_workspace);
+        for(int d = 0; d < ndms; ++d) {
+            SW_REQUIRE(h_d_out[d], "coherent dedispersion: null output for DM %d", d);
+            a.out[d] = static_cast<uint8_t*>(h_d_out[d]);
+        }
+        a.out_stride = out_row_stride;
+        a.dbg = reinterpret_cast<float2*>(d_debug_f32);
+        const int items = nstreams * nseg;
+        const size_t ws_items = std::min<size_t>(workspace_bytes / per_item, (size_t)items);
+        switch(fft_len / kSplitM) {
+        case 2: return launch_split<2>(a, items, ws_items, s);
+        case 4: return launch_split<4>(a, items, ws_items, s);
+        default: return launch_split<8>(a, items, ws_items, s);
+        }
+    }
+    Args a{};
+    a.in         = static_cast<const uint8_t*>(d_fpact_in);
+    a.row_stride = row_stride;
+    a.npa        = npol * nant;
+    a.nstreams   = nstreams;
+    a.nsamples   = nsamples;
+    a.overlap    = overlap;
+    a.lag        = lag;
+    a.nseg       = nseg;
+    a.ndms       = ndms;
+    a.chirp_dm_stride = (size_t)setup_nchans * fft_len;
+    a.tw         = tw;
+    a.chirp      = ch;
+    a.zero_flags = zero_flags;
+    for(int d = 0; d < ndms; ++d) {
+        SW_REQUIRE(h_d_out[d], "coherent dedispersion: null output for DM %d", d);
+        a.out[d] = static_cast<uint8_t*>(h_d_out[d]);
+    }
+    a.out_stride = out_row_stride;
+    a.dbg        = reinterpret_cast<float2*>(d_debug_f32);
+    switch(logn) {
+    case 8: return launch_logn<8>(a, s);
+    case 9: return launch_logn<9>(a, s);
+    case 10: return launch_logn<10>(a, s);
+    case 11: return launch_logn<11>(a, s);
+    case 12: return launch_logn<12>(a, s);
+    default: return launch_logn<13>(a, s);
+    }
+}
+
 }  // namespace cdd
 }  // namespace swb
 
@@ -896,7 +1003,8 @@ size_t sw_cdd_setup_bytes(int ndms, int nchans, int fft_len)
     if(logn < 8 || logn > 16 || ndms <= 0 || nchans <= 0) return 0;
     const Plan P = make_plan(logn > kSplitLog ? kSplitLog : logn);
     const size_t split_tw = logn > kSplitLog ? (size_t)fft_len : 0;
-    return ((size_t)P.tw_total + 16 + (size_t)ndms * nchans * fft_len + split_tw) * sizeof(c32);
+    return ((size_t)P.tw_total + kSetupGap + (size_t)ndms * nchans * fft_len + split_tw) *
+           sizeof(c32);
 }
 
 int sw_cdd_chirps(const float* h_dms, int ndms, int nchans, int fft_len,
@@ -910,15 +1018,14 @@ int sw_cdd_chirps(const float* h_dms, int ndms, int nchans, int fft_len,
     const int plog = logn > kSplitLog ? kSplitLog : logn;
     const Plan P = make_plan(plog);
     c32* tw = static_cast<c32*>(d_setup);
-    c32* ch = tw + P.tw_total + 16;  // keep the chirp table 128-byte aligned-ish
+    c32* ch = tw + P.tw_total + kSetupGap;
     twiddle_k<<<64, 256, 0, as_cuda(stream)>>>(tw, plog);
     SW_LAUNCH_CHECK();
-    // bit d of the word after the twiddle tables: DM d is exactly 0
-    uint32_t zero_mask = 0;
-    for(int d = 0; d < ndms && d < 32; ++d)
-        if(h_dms[d] == 0.0f) zero_mask |= 1u << d;
-    set_word_k<<<1, 1, 0, as_cuda(stream)>>>(reinterpret_cast<uint32_t*>(tw + P.tw_total),
-                                             zero_mask);
+    // the words after the twiddle tables flag the DMs of exactly 0
+    ZeroFlags zf{};
+    for(int d = 0; d < ndms; ++d) zf.f[d] = h_dms[d] == 0.0f ? 1u : 0u;
+    set_flags_k<<<1, kMaxDms, 0, as_cuda(stream)>>>(reinterpret_cast<uint32_t*>(tw + P.tw_total),
+                                                     zf);
     SW_LAUNCH_CHECK();
     SetupArgs S{};
     S.logn      = logn;
@@ -960,86 +1067,28 @@ int sw_coherent_dedisperse_ws(const void* d_fpact_in, size_t row_stride, int nch
                               size_t workspace_bytes, float* d_debug_f32,
                               sw_stream_t stream)
 {
-    const int logn = log2_exact(fft_len);
-    SW_REQUIRE(logn >= 8 && logn <= 16,
-               "coherent dedispersion: fft_len must be a power of two in [256, 65536]");
-    SW_REQUIRE(d_fpact_in && d_setup && h_d_out, "coherent dedispersion: null pointer");
-    SW_REQUIRE(ndms > 0 && ndms <= kMaxDms, "coherent dedispersion: 1..%d DMs", kMaxDms);
-    SW_REQUIRE(overlap >= 0 && overlap < fft_len,
-               "coherent dedispersion: overlap must be smaller than the FFT");
-    SW_REQUIRE(lag >= 0 && lag <= overlap,
-               "coherent dedispersion: the lag (%d) must lie in [0, overlap = %d]", lag, overlap);
-    SW_REQUIRE(nsamples > 0 && (size_t)overlap + nsamples <= row_stride,
-               "coherent dedispersion: input rows must hold history + gulp");
-    SW_REQUIRE((size_t)nsamples <= out_row_stride, "coherent dedispersion: output rows too short");
-    SW_REQUIRE(nchans > 0 && npol > 0 && nant > 0, "coherent dedispersion: empty shape");
-    const int plog = logn > kSplitLog ? kSplitLog : logn;
-    const Plan P = make_plan(plog);
-    const c32* tw = static_cast<const c32*>(d_setup);
-    const c32* ch = tw + P.tw_total + 16;
-    const int nstreams = nchans * npol * nant;
-    const int nseg = cdiv(nsamples, fft_len - overlap);
-    cudaStream_t s = as_cuda(stream);
-    if(logn > kSplitLog) {
-        const size_t per_item = (size_t)ndms * fft_len * sizeof(c32);
-        SW_REQUIRE(d_workspace && workspace_bytes >= per_item,
-                   "coherent dedispersion: fft_len %d needs a workspace of at least %zu bytes "
-                   "(sw_cdd_workspace_bytes)", fft_len, per_item);
-        SplitArgs a{};
-        a.in = static_cast<const uint8_t*>(d_fpact_in);
-        a.row_stride = row_stride;
-        a.nstreams = nstreams;
-        a.nsamples = nsamples;
-        a.overlap = overlap;
-        a.lag = lag;
-        a.nseg = nseg;
-        a.ndms = ndms;
-        a.npa = npol * nant;
-        a.tw = tw;
-        a.chirp = ch;
-        a.tws = ch + (size_t)ndms * nchans * fft_len;
-        a.z = static_cast<c32*>(d_workspace);
-        for(int d = 0; d < ndms; ++d) {
-            SW_REQUIRE(h_d_out[d], "coherent dedispersion: null output for DM %d", d);
-            a.out[d] = static_cast<uint8_t*>(h_d_out[d]);
-        }
-        a.out_stride = out_row_stride;
-        a.dbg = reinterpret_cast<float2*>(d_debug_f32);
-        const int items = nstreams * nseg;
-        const size_t ws_items = std::min<size_t>(workspace_bytes / per_item, (size_t)items);
-        switch(fft_len / kSplitM) {
-        case 2: return launch_split<2>(a, items, ws_items, s);
-        case 4: return launch_split<4>(a, items, ws_items, s);
-        default: return launch_split<8>(a, items, ws_items, s);
-        }
-    }
-    Args a{};
-    a.in         = static_cast<const uint8_t*>(d_fpact_in);
-    a.row_stride = row_stride;
-    a.npa        = npol * nant;
-    a.nstreams   = nstreams;
-    a.nsamples   = nsamples;
-    a.overlap    = overlap;
-    a.lag        = lag;
-    a.nseg       = nseg;
-    a.ndms       = ndms;
-    a.tw         = tw;
-    a.chirp      = ch;
-    a.zero_dms   = reinterpret_cast<const uint32_t*>(tw + P.tw_total);
-    for(int d = 0; d < ndms; ++d) {
-        SW_REQUIRE(h_d_out[d], "coherent dedispersion: null output for DM %d", d);
-        a.out[d] = static_cast<uint8_t*>(h_d_out[d]);
-    }
-    a.out_stride = out_row_stride;
-    a.dbg        = reinterpret_cast<float2*>(d_debug_f32);
-    switch(logn) {
-    case 8: return launch_logn<8>(a, s);
-    case 9: return launch_logn<9>(a, s);
-    case 10: return launch_logn<10>(a, s);
-    case 11: return launch_logn<11>(a, s);
-    case 12: return launch_logn<12>(a, s);
-    default: return launch_logn<13>(a, s);
-    }
+    SW_REQUIRE(d_setup, "coherent dedispersion: null setup");
+    return launch_cdd(d_fpact_in, row_stride, nchans, npol, nant, nsamples, fft_len, overlap,
+                      lag, d_setup, ndms, nchans, 0, 0, ndms, h_d_out, out_row_stride,
+                      d_workspace, workspace_bytes, d_debug_f32, stream);
+}
+
+int sw_coherent_dedisperse_channel(const void* d_fpact_in, size_t row_stride, int npol,
+                                   int nant, int nsamples, int fft_len, int overlap, int lag,
+                                   const void* d_setup, int setup_ndms, int setup_nchans,
+                                   int freq_idx, int dm_idx, void* d_out,
+                                   size_t out_row_stride, void* d_workspace,
+                                   size_t workspace_bytes, sw_stream_t stream)
+{
+    SW_REQUIRE(d_setup && d_out, "coherent dedispersion: null pointer");
+    SW_REQUIRE(setup_ndms > 0 && setup_nchans > 0 && freq_idx >= 0 && freq_idx < setup_nchans &&
+                   dm_idx >= 0 && dm_idx < setup_ndms,
+               "coherent dedispersion: channel %d / DM %d outside the setup (%d channels, %d DMs)",
+               freq_idx, dm_idx, setup_nchans, setup_ndms);
+    void* outs[1] = {d_out};
+    return launch_cdd(d_fpact_in, row_stride, 1, npol, nant, nsamples, fft_len, overlap, lag,
+                      d_setup, setup_ndms, setup_nchans, freq_idx, dm_idx, 1, outs,
+                      out_row_stride, d_workspace, workspace_bytes, nullptr, stream);
 }
 
 int sw_coherent_dedisperse(const void* d_fpact_in, size_t row_stride,

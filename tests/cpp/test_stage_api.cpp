@@ -42,6 +42,30 @@ static std::vector<int8_t> normal_int8(std::size_t n, float sigma, unsigned seed
     return v;
 }
 
+// host bytes <-> device described vectors
+template <typename V>
+static void put(V& v, const std::vector<int8_t>& h)
+{
+    EXPECT(v.size() * sizeof(typename V::value_type) == h.size());
+    cuda_check(cudaMemcpy(v.data(), h.data(), h.size(), cudaMemcpyHostToDevice), "put");
+}
+template <typename V>
+static std::vector<int8_t> bytes_of(const V& v)
+{
+    std::vector<int8_t> h(v.size() * sizeof(typename V::value_type));
+    cuda_check(cudaMemcpy(h.data(), v.data(), h.size(), cudaMemcpyDeviceToHost), "get");
+    return h;
+}
+template <typename T, typename V>
+static std::vector<T> values_of(const V& v)
+{
+    std::vector<T> h(v.size() * sizeof(typename V::value_type) / sizeof(T));
+    cuda_check(cudaMemcpy(h.data(), v.data(), h.size() * sizeof(T), cudaMemcpyDeviceToHost), "get");
+    return h;
+}
+
+using StokesI = SingleStokesBeamformerTraits<I>;
+
 static PipelineConfig base_config()
 {
     PipelineConfig c;
@@ -60,13 +84,17 @@ static void transposer_test()
         PipelineConfig c = base_config();
         const int A_in = p.first, H = p.second, F = (int)c.nchans(), A = (int)c.nantennas();
         auto h = normal_int8((std::size_t)H * A_in * F * 256 * 2 * 2, 40.0f, 1);
-        DeviceBuffer<int8_t> taftp, ftpa;
-        taftp.upload(h);
+        TAFTPVoltagesD<char2> taftp({(std::size_t)H, (std::size_t)A_in, (std::size_t)F, 256, 2});
+        taftp.tsamp(4096 / 856e6);
+        put(taftp, h);
+        FTPAVoltagesD<char2> ftpa;
         Transposer t(c);
         t.transpose(taftp, ftpa, A_in, nullptr);
         std::vector<int8_t> ref((std::size_t)F * H * 256 * 2 * A * 2);
         swo_transpose(h.data(), ref.data(), A_in, A, F, H, 256, 2);
-        EXPECT(ftpa.download() == ref);
+        EXPECT(bytes_of(ftpa) == ref);
+        EXPECT(ftpa.dims_as_string() == "FTPA" && ftpa.nsamples() == (std::size_t)H * 256);
+        EXPECT(ftpa.nantennas() == (std::size_t)A && ftpa.tsamp() == taftp.tsamp());
     }
     std::puts("PASS transposer");
 }
@@ -76,13 +104,14 @@ static void statistics_test()
     PipelineConfig c = base_config();
     const int F = 4, A = 64, T = 1024;
     auto h = normal_int8((std::size_t)F * T * 2 * A * 2, 20.0f, 1337);
-    DeviceBuffer<int8_t> ftpa;
-    ftpa.upload(h);
+    FTPAVoltagesD<char2> ftpa({(std::size_t)F, (std::size_t)T, 2, (std::size_t)A});
+    put(ftpa, h);
     StatisticsCalculator s(c, nullptr);
     s.calculate_statistics(ftpa);
     std::vector<float> ref((std::size_t)F * 2 * A * 4);
     swo_statistics(h.data(), ref.data(), F, T, 2, A);
-    auto got = s.statistics().download();
+    EXPECT(s.statistics().dims_as_string() == "FPA" && s.statistics().size() == (std::size_t)F * 2 * A);
+    auto got = values_of<float>(s.statistics());
     for(std::size_t i = 0; i < ref.size(); ++i)
         EXPECT(std::fabs(got[i] - ref[i]) <= 1e-5f * std::fabs(ref[i]) + 1e-6f);
     std::puts("PASS statistics");
@@ -94,18 +123,19 @@ static void weights_test()
     PipelineConfig c = base_config();
     const int A = 64, B = 128, F = 4;
     for(int which = 0; which < 3; ++which) {
-        std::vector<float> d((std::size_t)B * A * 3);
+        std::vector<float3> d((std::size_t)B * A);
         for(int i = 0; i < B * A; ++i) {
-            if(which == 0) { d[3 * i] = 1.0f; d[3 * i + 1] = 0.0f; d[3 * i + 2] = 0.0f; }
-            if(which == 1) { d[3 * i] = 1.0f; d[3 * i + 1] = 1e-11f; d[3 * i + 2] = 1e-10f; }
-            if(which == 2) { d[3 * i] = i * 1e-11f; d[3 * i + 1] = i * 1e-15f; d[3 * i + 2] = 0.0f; }
+            if(which == 0) d[i] = float3{1.0f, 0.0f, 0.0f};
+            if(which == 1) d[i] = float3{1.0f, 1e-11f, 1e-10f};
+            if(which == 2) d[i] = float3{i * 1e-11f, i * 1e-15f, 0.0f};
         }
-        DeviceBuffer<float> dd;
+        DeviceVector<float3> dd;
         dd.upload(d);
         WeightsManager wm(c, nullptr);
-        auto got = wm.weights(dd, 10.0, 9.0).download();
+        auto got = bytes_of(wm.weights(dd, 10.0, 9.0));
         std::vector<int8_t> ref((std::size_t)F * B * A * 2);
-        swo_weights(d.data(), ref.data(), c.channel_frequencies().data(), A, B, F, 10.0, 9.0, 0.0, 1);
+        swo_weights(reinterpret_cast<const float*>(d.data()), ref.data(),
+                    c.channel_frequencies().data(), A, B, F, 10.0, 9.0, 0.0, 1);
         EXPECT(got == ref);
     }
     std::puts("PASS weights");
@@ -119,8 +149,9 @@ static void beamformer_tests()
     c.output_level(32.0f);
     const int F = 4, A = 64, B = 128, T = 2048, ts = 16, S = 2;
     auto v = normal_int8((std::size_t)F * T * 2 * A * 2, 32.0f, 7);
-    DeviceBuffer<int8_t> ftpa;
-    ftpa.upload(v);
+    FTPAVoltagesD<char2> ftpa({(std::size_t)F, (std::size_t)T, 2, (std::size_t)A});
+    ftpa.tsamp(4096 / 856e6);
+    put(ftpa, v);
     const float level = 32.0f;
     const float ib_dof = 2.0f * ts * A * 2, cb_s = std::pow(127.0f * level * std::sqrt((float)A), 2);
     const float cb_dof = 2.0f * ts * 2;
@@ -129,19 +160,38 @@ static void beamformer_tests()
         cb_off(S * F, cb_s * cb_dof), bw(S * A, 1.0f);
     std::vector<int> mapping(B, 0);
     mapping[0] = 1;
-    DeviceBuffer<float> d_ibs, d_ibo, d_cbs, d_cbo, d_bw, raw;
-    DeviceBuffer<int> d_map;
-    DeviceBuffer<int8_t> ib, cb, w;
+    DeviceVector<float> d_ibs, d_ibo, d_cbs, d_cbo, d_bw;
+    DeviceVector<int> d_map;
     d_ibs.upload(ib_scale); d_ibo.upload(ib_off); d_cbs.upload(cb_scale); d_cbo.upload(cb_off);
     d_bw.upload(bw); d_map.upload(mapping);
-    IncoherentBeamformer ibf(c);
+    BTFPowersD<float> raw;
+    BTFPowersD<int8_t> ib;
+    IncoherentBeamformer<StokesI> ibf(c);
     ibf.beamform(ftpa, raw, ib, d_ibs, d_ibo, d_bw, S, nullptr);
     std::vector<float> raw_ref((std::size_t)S * (T / ts) * F);
     std::vector<int8_t> ib_ref(raw_ref.size());
     swo_ib(v.data(), raw_ref.data(), ib_ref.data(), F, ts, T, A, ib_scale.data(), ib_off.data(),
            bw.data(), S, 0);
-    EXPECT(raw.download() == raw_ref);
-    EXPECT(ib.download() == ib_ref);
+    EXPECT(values_of<float>(raw) == raw_ref);
+    EXPECT(bytes_of(ib) == ib_ref);
+    EXPECT(ib.dims_as_string() == "BTF" && ib.nbeams() == (std::size_t)S &&
+           std::fabs(ib.tsamp() - ts * ftpa.tsamp()) < 1e-15);
+    // full Stokes (FullStokesBeamformerTraits): component k of the float4 /
+    // char4 result is the single-Stokes result for parameter k
+    BTFPowersD<float4> raw4;
+    BTFPowersD<char4> ib4;
+    IncoherentBeamformer<FullStokesBeamformerTraits> ibf4(c);
+    ibf4.beamform(ftpa, raw4, ib4, d_ibs, d_ibo, d_bw, S, nullptr);
+    const auto r4 = values_of<float>(raw4);
+    const auto b4 = bytes_of(ib4);
+    for(int k = 0; k < 4; ++k) {
+        swo_ib(v.data(), raw_ref.data(), ib_ref.data(), F, ts, T, A, ib_scale.data(), ib_off.data(),
+               bw.data(), S, k);
+        for(std::size_t i = 0; i < raw_ref.size(); ++i) {
+            EXPECT(r4[4 * i + k] == raw_ref[i]);
+            EXPECT(b4[4 * i + k] == ib_ref[i]);
+        }
+    }
     std::puts("PASS incoherent_beamformer");
 
     std::mt19937 g(11);
@@ -152,14 +202,72 @@ static void beamformer_tests()
         hw[i]     = (int8_t)std::lround(127.0 * std::cos(th));
         hw[i + 1] = (int8_t)std::lround(127.0 * std::sin(th));
     }
-    w.upload(hw);
-    CoherentBeamformer cbf(c);
+    DeviceVector<char2> w((std::size_t)F * B * A);
+    cuda_check(cudaMemcpy(w.data(), hw.data(), hw.size(), cudaMemcpyHostToDevice), "weights");
+    TFBPowersD<int8_t> cb;
+    CoherentBeamformer<StokesI> cbf(c);
     cbf.beamform(ftpa, w, d_cbs, d_cbo, d_map, raw, cb, S, nullptr);
     std::vector<int8_t> cb_ref((std::size_t)(T / ts) * F * B);
     swo_cb(v.data(), hw.data(), cb_ref.data(), F, ts, T, B, A, cb_scale.data(), cb_off.data(),
            bw.data(), mapping.data(), 0, 1, nullptr);
-    EXPECT(cb.download() == cb_ref);
+    EXPECT(bytes_of(cb) == cb_ref);
+    EXPECT(cb.dims_as_string() == "TFB" && cb.nsamples() == (std::size_t)T / ts &&
+           cb.nbeams() == (std::size_t)B);
     std::puts("PASS coherent_beamformer");
+}
+
+// CoherentDedisperserTester.cu:21-204: the configuration of the reference's
+// fixture and its golden vector (DM 1000, one channel, 1024-point FFT), within
+// the reference's tolerance of one; DM 0 reproduces the input window.
+static void coherent_dedisperser_tests(const std::string& golden)
+{
+    const std::vector<float> dms = {0.0f, 1000.0f};
+    const std::size_t fft_length = 1024, nantennas = 64, nchans = 64, npols = 2;
+    const double tsamp = 4096 / 856e6, f_low = 856e6, bridge_bw = 13.375e6;
+    const double f2 = f_low + 856e6 / 4096;
+    const double delay = 4.148806423e15 * (1.0 / (f_low * f_low) - 1.0 / (f2 * f2)) * 1000.0;
+    const std::size_t max_delay_samps = (std::size_t)std::ceil(delay / tsamp);
+    EXPECT(max_delay_samps == 578);
+    CoherentDedisperserConfig cfg;
+    create_coherent_dedisperser_config(cfg, fft_length, max_delay_samps, nchans, npols, nantennas,
+                                       tsamp, f_low, bridge_bw, dms);
+    EXPECT(std::fabs(cfg.filter_delay - tsamp * 289) < 1e-15 && cfg.high_freq == f_low + bridge_bw);
+    CoherentDedisperser cdd(cfg);
+    std::ifstream fin(golden + "/codedisp_input_DM1000_1chan.bin", std::ios::binary);
+    std::ifstream fout(golden + "/codedisp_output_DM1000_1chan.bin", std::ios::binary);
+    std::vector<int8_t> in(1024 * 2 * 64 * 2), want(446 * 2 * 64 * 2);
+    fin.read(reinterpret_cast<char*>(in.data()), (std::streamsize)in.size());
+    fout.read(reinterpret_cast<char*>(want.data()), (std::streamsize)want.size());
+    EXPECT(fin.good() && fout.good());
+    TPAVoltagesD<char2> d_in({1024, npols, nantennas});
+    put(d_in, in);
+    FTPAVoltagesD<char2> d_out({1, fft_length - max_delay_samps, npols, nantennas});
+    cdd.dedisperse(d_in, d_out, 0, 1);
+    EXPECT(d_out.reference_dm() == 1000.0f);
+    const auto got = bytes_of(d_out);
+    std::size_t exact = 0;
+    for(std::size_t i = 0; i < got.size(); ++i) {
+        EXPECT(std::abs((int)got[i] - (int)want[i]) <= 1);
+        exact += got[i] == want[i];
+    }
+    std::printf("coherent dedisperser golden vector: %zu of %zu values exact\n", exact, got.size());
+    cdd.dedisperse(d_in, d_out, 0, 0);   // DM 0: the window's middle, unchanged
+    const auto id = bytes_of(d_out);
+    for(std::size_t i = 0; i < id.size(); ++i) EXPECT(id[i] == in[289 * 2 * 64 * 2 + i]);
+    // the gulp-length overload and its limit (CoherentDedisperser.cu:19-57)
+    PipelineConfig c = base_config();
+    c.nchans(64);
+    c.bandwidth(64 * 856e6 / 1024);
+    c.gulp_length_samps(65536);
+    c.ddplan().add_block(150.0f);
+    CoherentDedisperserConfig cfg2;
+    create_coherent_dedisperser_config(cfg2, c);
+    EXPECT(cfg2.fft_length == 65536 && cfg2.overlap_samps > 1000);
+    c.ddplan().add_block(5000.0f);
+    bool threw = false;
+    try { create_coherent_dedisperser_config(cfg2, c); } catch(const std::runtime_error&) { threw = true; }
+    EXPECT(threw);
+    std::puts("PASS coherent_dedisperser");
 }
 
 // IncoherentDedisperserTester.cu:39-126
@@ -181,16 +289,19 @@ static void incoherent_dedisperser_tests()
         EXPECT(d.max_sample_delay() > 0);
         std::size_t T = 3 * d.max_sample_delay();
         T -= (T - d.max_sample_delay()) % ts;
-        DeviceBuffer<int8_t> tfb, tdb;
+        DeviceVector<int8_t> tfb;
+        TDBPowersD<int8_t> tdb;
         tfb.upload(std::vector<int8_t>(T * c.nchans() * c.nbeams(), 1));
         d.dedisperse(tfb, tdb);
-        const auto out = tdb.download();
+        const auto out = bytes_of(tdb);
         EXPECT(out.size() == (T - d.max_sample_delay()) / ts * dms.size() * c.nbeams());
+        EXPECT(tdb.ndms() == dms.size() && tdb.nbeams() == c.nbeams());
         for(int8_t x : out) EXPECT(x == (int8_t)std::sqrt((double)(c.nchans() * ts)));
     }
     {
         IncoherentDedisperser d(c, dms);
-        DeviceBuffer<int8_t> tfb, tdb;
+        DeviceVector<int8_t> tfb;
+        TDBPowersD<int8_t> tdb;
         tfb.upload(std::vector<int8_t>(d.max_sample_delay() * c.nchans() * c.nbeams(), 0));
         bool threw = false;
         try { d.dedisperse(tfb, tdb); } catch(const std::runtime_error&) { threw = true; }
@@ -206,10 +317,11 @@ static void delay_manager_tests(const std::string& golden)
     c.delay_file(golden + "/test_delays.bin");
     DelayManager dm(c, nullptr);
     EXPECT(dm.nbeamsets() == 2);
-    EXPECT(dm.beamset_weights().size() == 2 * c.nantennas());
+    EXPECT(dm.beamset_weights_host().size() == 2 * c.nantennas());
     EXPECT(std::fabs(dm.epoch() - 1708082168.957) < 1e-3);
     const auto& d = dm.delays(dm.epoch() + 1.0);
-    EXPECT(d.size() == c.nbeams() * c.nantennas() * 3);
+    EXPECT(d.size() == c.nbeams() * c.nantennas());
+    EXPECT(dm.beamset_mapping().size() == c.nbeams() && dm.beamset_weights().size() == 2 * c.nantennas());
     bool threw = false;
     try { dm.delays(dm.epoch() - 10.0); } catch(const InvalidDelayEpoch&) { threw = true; }
     EXPECT(threw);
@@ -234,12 +346,39 @@ static void dedispersion_plan_tests()
     std::puts("PASS dedispersion_plan");
 }
 
-struct CountingHandler {
-    std::size_t calls = 0, bytes = 0;
-    void operator()(const int8_t*, std::size_t n, std::size_t) { ++calls; bytes += n; }
+// handlers with the reference's concept: init(header), operator()(vector, dm)
+struct CbCounter {
+    std::size_t inits = 0, calls = 0, bytes = 0;
+    std::vector<float> dms_seen;
+    double tsamp = 0.0, utc_offset = -1.0;
+    std::vector<double> freqs;
+    void init(const ObservationHeader&) { ++inits; }
+    void operator()(const TFBPowersD<int8_t>& v, std::size_t dm_idx)
+    {
+        ++calls;
+        bytes += v.size();
+        dms_seen.push_back(v.reference_dm());
+        EXPECT(v.dims_as_string() == "TFB" && dm_idx < 2);
+        tsamp = v.tsamp();
+        utc_offset = v.utc_offset();
+        freqs = v.frequencies();
+        (void)bytes_of(v);   // the view is readable on the legacy stream
+    }
+};
+struct IbCounter {
+    std::size_t inits = 0, calls = 0, nbeamsets = 0;
+    void init(const ObservationHeader&) { ++inits; }
+    void operator()(const BTFPowersD<int8_t>& v, std::size_t) { ++calls; nbeamsets = v.nbeams(); }
+};
+struct StatsCounter {
+    std::size_t inits = 0, calls = 0, nseries = 0;
+    void init(const ObservationHeader&) { ++inits; }
+    void operator()(const FPAStatsD<Statistics>& v) { ++calls; nseries = v.size(); }
 };
 
-// BeamformerPipelineTester.cu:119-167 (zeros through the full chain)
+// BeamformerPipelineTester.cu:119-167 (zeros through the full chain) with the
+// reference's handler concept and epoch arithmetic (BeamformerPipeline.cu:
+// 100-115, 262-301)
 static void pipeline_smoke(const std::string& golden)
 {
     PipelineConfig c = base_config();
@@ -247,25 +386,36 @@ static void pipeline_smoke(const std::string& golden)
     c.gulp_length_samps(4096);
     c.ddplan().add_block(0.0f);
     c.ddplan().add_block(5.0f);
-    CountingHandler h;
-    BeamformerPipeline<CountingHandler> pipe(c, h, 57);
-    std::vector<int8_t> taftp((std::size_t)16 * 57 * c.nchans() * 256 * 2 * 2, 0);
-    for(int g = 0; g < 3; ++g) pipe(taftp.data(), 1708082168.957 + 1.0 + g * 0.02);
-    EXPECT(h.calls == 6);
-    EXPECT(h.bytes == 6 * (4096 / 16) * c.nchans() * c.nbeams());
-    // DescribedVector metadata of the outputs (CoherentBeamformer.cu:231-235)
-    const Description d = pipe.describe_cb(1);
-    EXPECT(d.dims_as_string() == "TFB");
-    EXPECT(d.extents() == std::vector<std::size_t>({4096 / 16, c.nchans(), c.nbeams()}));
-    EXPECT(d.nsamples() == 4096 / 16 && d.nchannels() == c.nchans() && d.nbeams() == c.nbeams());
-    EXPECT(d.frequencies() == c.channel_frequencies());
+    CbCounter cbh;
+    IbCounter ibh;
+    StatsCounter sh;
+    {
+        BeamformerPipeline<CbCounter, IbCounter, StatsCounter> pipe(c, cbh, ibh, sh);
+        ObservationHeader hdr{};
+        hdr.nantennas = 57;
+        hdr.utc_start = 1708082168.957 + 1.0;
+        hdr.sample_clock = 1712e6;
+        pipe.init(hdr, 0.0);
+        EXPECT(cbh.inits == 1 && ibh.inits == 1 && sh.inits == 1);
+        TAFTPVoltagesH<char2> taftp({16, 57, c.nchans(), 256, 2});
+        std::memset(taftp.data(), 0, taftp.size() * sizeof(char2));
+        for(int g = 0; g < 3; ++g) EXPECT(pipe(taftp) == false);
+        EXPECT(cbh.calls == 4);   // gulps 0 and 1 delivered, gulp 2 pending
+        pipe.flush();
+        EXPECT(pipe.call_count() == 3);
+    }
+    EXPECT(cbh.calls == 6 && ibh.calls == 6 && sh.calls == 3);
+    EXPECT(cbh.bytes == 6 * (4096 / 16) * c.nchans() * c.nbeams());
+    EXPECT(cbh.dms_seen[0] == 0.0f && cbh.dms_seen[1] == 5.0f);
+    EXPECT(cbh.freqs == c.channel_frequencies());
     const double chan_tsamp = (double)c.nchans() / c.bandwidth();
-    EXPECT(std::fabs(d.tsamp() - 16 * chan_tsamp) < 1e-15);
-    EXPECT(d.reference_dm() == 5.0f && d.utc_offset() >= 0.0);
-    const Description ib = pipe.describe_ib(0);
-    EXPECT(ib.dims_as_string() == "BTF" && ib.nsamples() == 4096 / 16);
+    EXPECT(std::fabs(cbh.tsamp - 16 * chan_tsamp) < 1e-15 && cbh.utc_offset >= 0.0);
+    EXPECT(ibh.nbeamsets == 2 && sh.nseries == c.nchans() * 2 * c.nantennas());
+    // a pipeline used before init() refuses the gulp
+    BeamformerPipeline<CbCounter, IbCounter, StatsCounter> pipe2(c, cbh, ibh, sh);
+    TAFTPVoltagesH<char2> taftp({16, 57, c.nchans(), 256, 2});
     bool threw = false;
-    try { pipe.describe_cb(2); } catch(const std::runtime_error&) { threw = true; }
+    try { pipe2(taftp); } catch(const std::runtime_error&) { threw = true; }
     EXPECT(threw);
     std::puts("PASS beamformer_pipeline");
 }
@@ -273,14 +423,17 @@ static void pipeline_smoke(const std::string& golden)
 struct TdbCollector {
     std::vector<std::vector<int8_t>> got[2];
     std::size_t nbeams = 0, ndms[2] = {0, 0};
-    void operator()(const int8_t* d_tdb, std::size_t nout, std::size_t ndm, std::size_t nb,
-                    std::size_t block)
+    float ref_dm[2] = {0, 0};
+    double utc_offset[2] = {0, 0};
+    void init(const ObservationHeader&) {}
+    void operator()(const TDBPowersD<int8_t>& tdb, std::size_t block)
     {
-        std::vector<int8_t> h(nout * ndm * nb);
-        cuda_check(cudaMemcpy(h.data(), d_tdb, h.size(), cudaMemcpyDeviceToHost), "tdb");
-        got[block].push_back(std::move(h));
-        nbeams = nb;
-        ndms[block] = ndm;
+        got[block].push_back(bytes_of(tdb));
+        nbeams = tdb.nbeams();
+        ndms[block] = tdb.ndms();
+        EXPECT(tdb.dms().size() == tdb.ndms());
+        ref_dm[block] = tdb.reference_dm();
+        utc_offset[block] = tdb.utc_offset();
     }
 };
 
@@ -295,18 +448,21 @@ static void idd_pipeline_tests()
     c.bandwidth(32e6);
     c.centre_frequency(580e6);
     c.cb_tscrunch(16);
-    DedispersionPlan plan;
-    plan.add_block("5.0:0.0:20.0:5.0:1");
-    plan.add_block("30.0:25.0:45.0:10.0:2");
+    c.ddplan().add_block("5.0:0.0:20.0:5.0:1");
+    c.ddplan().add_block("30.0:25.0:45.0:10.0:2");
+    const auto& plan = c.ddplan();
     TdbCollector col;
-    IncoherentDedispersionPipeline<TdbCollector> idd(c, plan, col);
+    IncoherentDedispersionPipeline<int8_t, int8_t, TdbCollector> idd(c, col);
     const std::size_t T = 40000, slot = c.nchans() * c.nbeams();
-    DeviceBuffer<int8_t> ones;
+    DeviceVector<int8_t> ones;
     ones.upload(std::vector<int8_t>(T * slot, 1));
+    const double tsamp = 16 / (32e6 / 64);
     for(int b = 0; b < 2; ++b) {
         std::size_t pos = 0;
         for(std::size_t n : {1000u, 17u, 20000u, 18983u}) {
-            idd(ones.data() + pos * slot, n, b);
+            auto v = TFBPowersD<int8_t>::view(ones.data() + pos * slot, {n, c.nchans(), c.nbeams()});
+            v.tsamp(tsamp);
+            idd(v, b);
             pos += n;
         }
         EXPECT(pos == T);
@@ -320,6 +476,8 @@ static void idd_pipeline_tests()
         D -= D % ts;
         EXPECT(col.got[b].size() == (T - O) / D);
         EXPECT(col.ndms[b] == plan[b].incoherent_dms.size());
+        EXPECT(col.ref_dm[b] == plan[b].coherent_dm);
+        EXPECT(std::fabs(col.utc_offset[b] - O * tsamp) < 1e-12);
         const int8_t want = (int8_t)std::sqrt((double)(c.nchans() * ts));
         for(const auto& v : col.got[b]) {
             EXPECT(v.size() == D / ts * col.ndms[b] * c.nbeams());
@@ -395,6 +553,7 @@ int main(int argc, char** argv)
     statistics_test();
     weights_test();
     beamformer_tests();
+    coherent_dedisperser_tests(golden);
     incoherent_dedisperser_tests();
     delay_manager_tests(golden);
     dedispersion_plan_tests();
