@@ -110,14 +110,15 @@ transpose_fpact_k(const uint4* __restrict__ taftp, uint8_t* __restrict__ fpact,
 }
 
 // FTPA <-> FPACT converters (reference-layout stage wrappers and tests).
-// One thread per 4 consecutive samples of one planar row.
+// One thread per 4 consecutive samples of one planar row (fewer in the last
+// group when nsamples is not a multiple of 4).
 __global__ void ftpa_to_fpact_k(const int8_t* __restrict__ ftpa,
                                 int8_t* __restrict__ fpact, int nchans,
                                 int nsamples, int nant, size_t row_stride,
                                 size_t sample_offset, int to_fpact)
 {
     const size_t nrows  = (size_t)nchans * kPol * nant * 2;
-    const size_t nquads = nrows * (nsamples / 4);
+    const size_t nquads = nrows * ((nsamples + 3) / 4);
     for(size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nquads;
         i += (size_t)gridDim.x * blockDim.x) {
         const size_t row = i % nrows;  // row fastest -> coalesced FTPA reads
@@ -129,6 +130,7 @@ __global__ void ftpa_to_fpact_k(const int8_t* __restrict__ ftpa,
         int8_t* prow = fpact + row * row_stride + sample_offset + t;
 #pragma unroll
         for(int k = 0; k < 4; ++k) {
+            if(t + k >= nsamples) break;  // ragged last group
             const size_t fi = ((((size_t)f * nsamples + t + k) * kPol + p) * nant + a) * 2 + c;
             if(to_fpact) prow[k] = ftpa[fi];
             else const_cast<int8_t*>(ftpa)[fi] = prow[k];
@@ -214,9 +216,9 @@ static int convert(const void* ftpa, void* fpact, int nchans, int nsamples,
                    int to_fpact)
 {
     SW_REQUIRE(ftpa && fpact, "FTPA/FPACT conversion: null pointer");
-    SW_REQUIRE(nsamples % 4 == 0, "FTPA/FPACT conversion: nsamples must be a multiple of 4");
+    SW_REQUIRE(nsamples > 0 && nchans > 0 && nant > 0, "FTPA/FPACT conversion: empty shape");
     SW_REQUIRE(off + nsamples <= row_stride, "FTPA/FPACT conversion: rows too short");
-    const size_t work = (size_t)nchans * kPol * nant * 2 * (nsamples / 4);
+    const size_t work = (size_t)nchans * kPol * nant * 2 * ((nsamples + 3) / 4);
     ftpa_to_fpact_k<<<grid_for(work, 256), 256, 0, as_cuda(stream)>>>(
         static_cast<const int8_t*>(ftpa), static_cast<int8_t*>(fpact), nchans,
         nsamples, nant, row_stride, off, to_fpact);
