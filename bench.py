@@ -439,8 +439,14 @@ def main_b200(args):
             "kernels": kern, "roofline": roof, "hbm_peak_gbs": hbm_peak, "e2e": e2e,
             "cdd_plan": plan_dev,
             "gpu_launches": launches * args.steps, "clocks": clocks}
+    pipe_out_tfb = pipe.cb_device(0).clone() if world > 1 else None
     pipe.close()
     line["long_fft"] = long_fft
+    if world > 1:
+        try:   # every rank takes the same steps; a failure is reported, not fatal
+            line["chain"] = chain_case(torch, stages, pipe_out_tfb, rank, world, args.steps)
+        except Exception as e:  # noqa: BLE001
+            line["chain"] = {"error": f"{type(e).__name__}: {e}"}
     if not args.no_uhf:
         free, _ = torch.cuda.mem_get_info()
         if free >= 120e9:   # the UHF chain holds ~100 GB (aggregation buffers included)
@@ -553,6 +559,59 @@ def cdd_window_deviation(torch, stages, taftp, centre, bwidth, fft_len, overlap,
         res["per_dm"][str(dm)] = {"mismatch_fraction": float(np.mean(fr)), "max_lsb": mx}
     torch.cuda.synchronize()
     return res
+
+
+def chain_case(torch, stages, tfb, rank, world, K):
+    """The channel-partitioned chain after beamforming (N > 1): this rank's
+    DM-0 coherent beams of its subband, TFB [4096][64][1024], go through one
+    NCCL all-to-all (subbands.channels_to_beams: device tensors, no TMA) to
+    [4096][64 x world][1024 / world], then the device incoherent dedisperser
+    sums this rank's beam block over the whole band for 32 trial DMs 0-10.
+    Timed with CUDA events, max over ranks."""
+    from skyweaver_b200 import subbands
+    import torch.distributed as dist
+    F, ts = WORK["nchans"], WORK["tscrunch"]
+    Ftot = F * world
+    bw = Ftot * WORK["chbw"]
+    freqs = stages.channel_frequencies(WORK["centre"], bw, Ftot)
+    trials = np.linspace(0.0, 10.0, 32).astype(np.float32)
+    tsamp_cb = ts / WORK["chbw"]
+    k = 4.148806423e15
+    delays = np.array([[int(k * (1 / freqs[0] ** 2 - 1 / f ** 2) * d / tsamp_cb + 0.5)
+                        for f in freqs] for d in trials], np.int32)
+    maxd = int(delays.max())
+    n = tfb.shape[0]
+    if maxd >= n:
+        return {"skipped": f"max delay {maxd} exceeds the {n} samples of a gulp"}
+    d_delays = torch.from_numpy(delays).cuda()
+    scale = float(np.float32(np.sqrt(Ftot)))
+    stream = torch.cuda.current_stream()
+
+    def step():
+        blk = subbands.channels_to_beams(tfb)
+        return blk, stages.incoherent_dedisperse(blk[:n], d_delays, maxd, 1, scale)
+
+    for _ in range(2):
+        step()
+    torch.cuda.synchronize()
+    dist.barrier()
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    xs, ids = 0.0, 0.0
+    for _ in range(K):
+        e0.record(stream)
+        blk = subbands.channels_to_beams(tfb)
+        e1.record(stream)
+        stages.incoherent_dedisperse(blk[:n], d_delays, maxd, 1, scale)
+        e2.record(stream)
+        torch.cuda.synchronize()
+        xs += e0.elapsed_time(e1)
+        ids += e1.elapsed_time(e2)
+    xs = max_over_ranks(xs / K, world, "cuda")
+    ids = max_over_ranks(ids / K, world, "cuda")
+    return {"workload": f"DM-0 beams of {world} subbands: all-to-all to beam blocks, then "
+                        f"incoherent dedispersion over {Ftot} channels, 32 trial DMs 0-10",
+            "exchange_ms": xs, "exchange_bytes_per_rank": int(tfb.numel()),
+            "idd_ms": ids, "max_delay_samples": maxd}
 
 
 RAGGED = dict(nant=64, nchans=64, gulp=32768, tscrunch=16, dms=[0.0, 50.0, 150.0, 500.0],

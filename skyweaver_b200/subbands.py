@@ -45,3 +45,30 @@ def channels_to_beams(tfb, group=None):
     dist.all_to_all_single(recv, send, group=group)
     # recv[src] = [T][F_local][B / world] of the source rank's channel block
     return recv.movedim(0, 1).reshape(T, world * F, B // world, *rest)
+
+
+class ChannelChain:
+    """One rank's part of the channel-partitioned chain:
+
+        beamform this rank's channel block  ->  channels_to_beams (one
+        all-to-all)  ->  incoherent dedispersion of this rank's beam block
+        over every channel
+
+    `beamform(voltages)` returns the coherent beams of the rank's channels,
+    TFB [T][F_local][B] (e.g. a BeamformerPipeline's device output);
+    `dedisperse(tfb)` takes [T][F_total][B / world] and returns the rank's
+    dedispersed beams (e.g. stages.incoherent_dedisperse with the whole
+    band's delays, or an IncoherentDedispersionPipeline push).  The stages
+    stay on the rank's device; the only collective is the exchange.  The
+    reference instead runs one process per bridge and dedisperses each
+    bridge on its own channels (MultiBeamWriter.hpp:18-40,
+    detail/IncoherentDedispersionPipeline.cu:6-113)."""
+
+    def __init__(self, beamform, dedisperse, group=None):
+        self.beamform = beamform
+        self.dedisperse = dedisperse
+        self.group = group
+
+    def __call__(self, voltages):
+        tfb = self.beamform(voltages)
+        return self.dedisperse(channels_to_beams(tfb, self.group))

@@ -142,3 +142,77 @@ def test_channel_partition_exchange_to_beam_blocks(tmp_path, oracle):
         bs = subbands.rank_beams(B, world, r)
         assert np.array_equal(np.load(tmp_path / f"beams{r}.npy"), full[:, :, bs])
         assert np.array_equal(np.load(tmp_path / f"tdb{r}.npy"), ref[:, :, bs])
+
+
+def _chain_case(oracle, F=8, A=8, B=12, T=2048, ts=4, seed=33):
+    """A small seeded gulp, its weights and the whole band's incoherent
+    dedispersion delays (the same on every rank)."""
+    from skyweaver_b200 import synthetic
+    g = synthetic.rng(seed)
+    chbw = 856e6 / 1024
+    freqs = 1284e6 + (np.arange(F) - F / 2 + 0.5) * chbw
+    ftpa = np.clip(np.rint(g.normal(0, 8, size=(F, T, 2, A, 2))), -127, 127).astype(np.int8)
+    w = oracle.weights(synthetic.delay_model(g, B, A), freqs, 0.0, 0.0)
+    delays, maxd = oracle.idd_delays(freqs, np.array([0, 20, 40], np.float32), ts / chbw)
+    assert 0 < maxd < T // ts
+    return ftpa, w, delays, maxd
+
+
+def _beams(oracle, ftpa, w, ts):
+    F, A = ftpa.shape[0], ftpa.shape[3]
+    one = np.ones(F, np.float32)
+    return oracle.coherent_beam(ftpa, w, ts, one * 1e4, one * 0, np.ones((1, A), np.float32),
+                                np.zeros(w.shape[1], np.int32))
+
+
+def _chain_main(rank, world, port, out_dir):
+    import torch
+    import torch.distributed as dist
+    sys.path.insert(0, REPO)
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    from skyweaver_b200 import subbands
+    import swb_oracle as oracle
+    oracle.build()
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
+                            world_size=world)
+    try:
+        ftpa, w, delays, maxd = _chain_case(oracle)
+        F, ts = ftpa.shape[0], 4
+        ch = subbands.rank_channels(F, world, rank)
+        # each rank holds only its channels' voltages and weights
+        mine = np.ascontiguousarray(ftpa[ch])
+        w_mine = np.ascontiguousarray(w[ch])
+
+        def beamform(v):
+            return torch.from_numpy(_beams(oracle, v, w_mine, ts))
+
+        def dedisperse(tfb):
+            x = tfb.numpy()
+            n = x.shape[0]
+            return oracle.idd(np.ascontiguousarray(x[:n]), delays, maxd, 1, np.float32(3.0))
+
+        chain = subbands.ChannelChain(beamform, dedisperse)
+        np.save(os.path.join(out_dir, f"chain{rank}.npy"), chain(mine))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_channel_partitioned_chain_equals_single_process(tmp_path, oracle):
+    """The whole chain on two gloo ranks (beamform own channels -> all-to-all
+    -> incoherent dedispersion of own beams over the whole band) equals the
+    single-process chain (beamform every channel -> dedisperse) sliced by
+    beam block."""
+    import torch.multiprocessing as mp
+    world = 2
+    mp.start_processes(_chain_main, args=(world, _free_port(), str(tmp_path)), nprocs=world,
+                       join=True, start_method="spawn")
+    sys.path.insert(0, REPO)
+    from skyweaver_b200 import subbands
+    ftpa, w, delays, maxd = _chain_case(oracle)
+    full = _beams(oracle, ftpa, w, 4)
+    ref = oracle.idd(np.ascontiguousarray(full), delays, maxd, 1, np.float32(3.0))
+    B = w.shape[1]
+    for r in range(world):
+        got = np.load(tmp_path / f"chain{r}.npy")
+        assert np.array_equal(got, ref[:, :, subbands.rank_beams(B, world, r)])
