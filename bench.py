@@ -335,7 +335,10 @@ def main_b200(args):
     common = dict(nantennas=A, input_nantennas=A, nchans=F, nbeams=B, gulp_samples=T,
                   tscrunch=ts, centre_frequency=centre, bandwidth=bwidth, dms=dms,
                   beamset_weights=bwts, beamset_mapping=mapping)
-    pipe = stages.BeamformerPipeline(**common, grouped=True, use_graph=True)
+    # the autotuner picks the FFT length, the beamformer's work-item size and
+    # its pipeline depths for this shape (cached for the process)
+    tune = stages.autotune(A, B, F, T, ts, dms, centre, bwidth)
+    pipe = stages.BeamformerPipeline(**common, grouped=True, use_graph=True, autotune=True)
     pipe.set_delays(delays, 1.7e9)
     fft_len, overlap, lag = pipe.cdd_plan()
     epoch0 = 1.7e9
@@ -368,7 +371,7 @@ def main_b200(args):
     value = rtf * world
 
     # ---- plain GPU form: one CB launch per (DM, beamset), no graph
-    plain = stages.BeamformerPipeline(**common, grouped=False, use_graph=False)
+    plain = stages.BeamformerPipeline(**common, grouped=False, use_graph=False, autotune=True)
     plain.set_delays(delays, 1.7e9)
     ms_plain = time_steps(lambda i: plain.process_device(gulp(i), epoch0 + i * gulp_s),
                           max(3, args.steps // 2), 2)
@@ -377,7 +380,7 @@ def main_b200(args):
 
     # ---- per-kernel timings (CUDA events on the launching stream)
     kern = kernel_breakdown(torch, stages, taftp, delays, fft_len, overlap, lag, centre,
-                            bwidth, args.steps)
+                            bwidth, args.steps, tune)
     # ---- the plan's deviation from 65536-point (= gulp) windows, the
     # reference's FFT length
     plan_dev = cdd_window_deviation(torch, stages, taftp, centre, bwidth, fft_len, overlap, lag)
@@ -438,6 +441,8 @@ def main_b200(args):
             "batched_vs_plain": ms_plain / ms_graph, "ragged": ragged,
             "kernels": kern, "roofline": roof, "hbm_peak_gbs": hbm_peak, "e2e": e2e,
             "cdd_plan": plan_dev,
+            "autotune": {k: tune[k] for k in ("fft_len", "cb_tiles_per_item", "cb_voltage_stages",
+                                              "cb_weight_stages")},
             "gpu_launches": launches * args.steps, "clocks": clocks}
     pipe_out_tfb = pipe.cb_device(0).clone() if world > 1 else None
     pipe.close()
@@ -462,7 +467,8 @@ def main_b200(args):
         dist.destroy_process_group()
 
 
-def kernel_breakdown(torch, stages, taftp, delays, fft_len, overlap, lag, centre, bwidth, K):
+def kernel_breakdown(torch, stages, taftp, delays, fft_len, overlap, lag, centre, bwidth, K,
+                     tune):
     """Each stage timed standalone with CUDA events over K launches."""
     A, B, F, T, ts = WORK["nant"], WORK["nbeams"], WORK["nchans"], WORK["gulp"], WORK["tscrunch"]
     dms = WORK["dms"]
@@ -510,7 +516,10 @@ def kernel_breakdown(torch, stages, taftp, delays, fft_len, overlap, lag, centre
     scl = dev(np.full(F, 1e9, np.float32))
     cbo = [torch.empty((T // ts, F, B), dtype=torch.int8, device="cuda") for _ in dms]
     probs = [(o, c, r, 0, B) for o, c, r in zip(outs, cbo, raws[:len(dms)])]
-    ms = timeit(lambda: stages.coherent_beamform_grouped(probs, gemm, scl, scl, mapping, T, ts))
+    cbt = dict(tiles_per_item=tune["cb_tiles_per_item"], voltage_stages=tune["cb_voltage_stages"],
+               weight_stages=tune["cb_weight_stages"])
+    ms = timeit(lambda: stages.coherent_beamform_grouped(probs, gemm, scl, scl, mapping, T, ts,
+                                                         **cbt))
     ops = 8.0 * A * B * 2 * F * T * len(dms)
     out["coherent_beamformer"] = {"ms": ms, "tops": ops / (ms * 1e-3) / 1e12,
                                   "ops_per_launch": ops}

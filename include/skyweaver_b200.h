@@ -215,6 +215,8 @@ typedef struct sw_cb_shape {
     size_t row_stride;  /* FPACT row stride (samples)                     */
     size_t sample_offset;
     int tiles_per_item; /* 64-sample tiles per work item (0: 64; see sw_autotune) */
+    int voltage_stages; /* voltage tiles in flight, 2..8 (0: 4; see sw_autotune) */
+    int weight_stages;  /* weight blocks in flight, 2..3 (0: 2)                  */
 } sw_cb_shape;
 
 /* Replaces CoherentBeamformer<BfTraits>::beamform
@@ -377,10 +379,11 @@ int sw_idd_pipeline_geometry(const sw_idd_pipeline* p, int block,
 /* Autotuner                                                            */
 /* ------------------------------------------------------------------ */
 /* Times the coherent dedisperser at every FFT length the DM smear allows
- * and the coherent beamformer at several work-item sizes, on synthetic data
- * of this exact shape, and returns the fastest choice (cached per key
- * (nantennas, nbeams, nchans, nsamples, tscrunch, ndms, overlap) for the
- * process). The reference's launch shapes are compile-time constants
+ * and the coherent beamformer at several work-item sizes (its tile shape in
+ * time) and pipeline depths (voltage and weight copies in flight), on
+ * synthetic data of this exact shape, and returns the fastest choice (cached
+ * per key (nantennas, nbeams, nchans, nsamples, tscrunch, ndms, overlap) for
+ * the process). The reference's launch shapes are compile-time constants
  * (skyweaver_constants.hpp:28-135); this has no counterpart there. Needs a
  * few GB of device memory while it runs. */
 typedef struct sw_tuning {
@@ -389,6 +392,8 @@ typedef struct sw_tuning {
     int lag;                /* of it, trimmed at each window's end       */
     int cb_tiles_per_item;  /* sw_cb_shape.tiles_per_item                */
     float cdd_ms, cb_ms;    /* measured per gulp at the chosen settings  */
+    int cb_voltage_stages;  /* sw_cb_shape.voltage_stages                */
+    int cb_weight_stages;   /* sw_cb_shape.weight_stages                 */
 } sw_tuning;
 
 int sw_autotune(int nantennas, int nbeams, int nchans, int nsamples,

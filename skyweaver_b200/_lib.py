@@ -39,7 +39,8 @@ class CbShape(ctypes.Structure):
     _fields_ = [("nchans", c_int), ("nsamples", c_int), ("nantennas", c_int),
                 ("nbeams", c_int), ("tscrunch", c_int), ("stokes", c_int),
                 ("ib_subtract", c_int), ("row_stride", c_size_t),
-                ("sample_offset", c_size_t), ("tiles_per_item", c_int)]
+                ("sample_offset", c_size_t), ("tiles_per_item", c_int),
+                ("voltage_stages", c_int), ("weight_stages", c_int)]
 
 
 class PipelineConfig(ctypes.Structure):
@@ -56,7 +57,8 @@ class PipelineConfig(ctypes.Structure):
 
 class Tuning(ctypes.Structure):
     _fields_ = [("fft_len", c_int), ("overlap", c_int), ("lag", c_int), ("cb_tiles_per_item", c_int),
-                ("cdd_ms", c_float), ("cb_ms", c_float)]
+                ("cdd_ms", c_float), ("cb_ms", c_float), ("cb_voltage_stages", c_int),
+                ("cb_weight_stages", c_int)]
 
 
 _SIGS = {

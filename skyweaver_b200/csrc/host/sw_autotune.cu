@@ -1,8 +1,10 @@
 // Autotuner for the per-gulp chain, keyed on (nantennas, nbeams, nchans,
 // nsamples, tscrunch, DM set): times the coherent dedisperser at every FFT
-// length that fits the DM smear and the coherent beamformer at several
-// work-item sizes on synthetic int8 data of that exact shape, and caches the
-// fastest choice per key for the life of the process.
+// length that fits the DM smear, and the coherent beamformer at several
+// work-item sizes (the extent of its tiles in time) and then several
+// pipeline depths (voltage and weight copies in flight) on synthetic int8
+// data of that exact shape, and caches the fastest choice per key for the
+// life of the process.
 //
 // The reference has no autotuner (its kernel shapes are compile-time
 // constants, skyweaver_constants.hpp:28-135); it is what picks the B200
@@ -167,23 +169,39 @@ extern "C" int sw_autotune(int nantennas, int nbeams, int nchans, int nsamples, 
         SW_CUDA_CHECK(cudaStreamSynchronize(s));
     }
     best.cb_ms = 1e30f;
-    for(int tpi : {4, 8, 16, 32, 64, 128}) {
-        if(tpi > T / 64 && tpi != 4) break;
-        sw_cb_shape shape{F, T, A, nbeams, ts, 0, 1, (size_t)T, 0, tpi};
+    auto time_cb = [&](int tpi, int vst, int wst, float* ms) {
+        sw_cb_shape shape{F, T, A, nbeams, ts, 0, 1, (size_t)T, 0, tpi, vst, wst};
         std::vector<sw_cb_problem> probs;
         for(int d = 0; d < ndm; ++d)
             probs.push_back({dd[d], static_cast<int8_t*>(cb.p) + (size_t)d * nout * F * nbeams,
                              static_cast<float*>(ib.p), 0, nbeams});
-        float ms = 0.0f;
-        SW_TRY(time_ms([&] {
+        return time_ms([&] {
             return sw_coherent_beamform_grouped(&shape, probs.data(), ndm, wgemm.p,
                                                 static_cast<float*>(scl.p),
                                                 static_cast<float*>(scl.p),
                                                 static_cast<int*>(map.p), stream);
-        }, s, 3, &ms));
+        }, s, 3, ms);
+    };
+    // work-item size (the tile's extent in time) at the default depths ...
+    for(int tpi : {4, 8, 16, 32, 64, 128}) {
+        if(tpi > T / 64 && tpi != 4) break;
+        float ms = 0.0f;
+        SW_TRY(time_cb(tpi, 4, 2, &ms));
         if(ms < best.cb_ms) {
             best.cb_ms = ms;
             best.cb_tiles_per_item = tpi;
+            best.cb_voltage_stages = 4;
+            best.cb_weight_stages = 2;
+        }
+    }
+    // ... then the pipeline depths at that size
+    for(auto vw : {std::pair<int, int>{2, 2}, {3, 2}, {6, 2}, {8, 2}, {4, 3}, {6, 3}}) {
+        float ms = 0.0f;
+        SW_TRY(time_cb(best.cb_tiles_per_item, vw.first, vw.second, &ms));
+        if(ms < best.cb_ms) {
+            best.cb_ms = ms;
+            best.cb_voltage_stages = vw.first;
+            best.cb_weight_stages = vw.second;
         }
     }
     SW_CUDA_CHECK(cudaStreamSynchronize(s));

@@ -78,6 +78,7 @@ struct sw_pipeline {
     int fft_len = 0, overlap = 0;  // overlap: multiple of 16
     int lag = 0;                   // of it, trimmed at each window's end
     int cb_tpi = 0;                // CB work-item size (0: kernel default)
+    int cb_vst = 0, cb_wst = 0;    // CB pipeline depths (0: kernel defaults)
     size_t ext_stride = 0, ext_off = 0, dd_stride = 0;
     size_t v_off = 0;           // first sample of the beamformers' voltages in a row
     std::vector<int> dd_of;     // per DM: index into dd (-1: DM 0, read from ext)
@@ -168,6 +169,8 @@ int sw_pipeline::init(const sw_pipeline_config& c)
                                &tu, nullptr));
             fft_len = tu.fft_len;
             cb_tpi = tu.cb_tiles_per_item;
+            cb_vst = tu.cb_voltage_stages;
+            cb_wst = tu.cb_weight_stages;
         } else {
             fft_len = swb::cdd_model_fft_len(overlap);
         }
@@ -305,7 +308,8 @@ int sw_pipeline::enqueue_chain(const void* d_in, int parity, bool first)
                                                ib_raw[parity][d].as<float>(),
                                                ib_i8[parity][d].as<int8_t>(), s, chan_order));
     }
-    sw_cb_shape shape{F, T, A, B, ts, cfg.stokes, cfg.ib_subtract, vstride, voff, cb_tpi};
+    sw_cb_shape shape{F,     T,    A,    B,      ts,     cfg.stokes, cfg.ib_subtract,
+                      vstride, voff, cb_tpi, cb_vst, cb_wst};
     if(cfg.grouped) {
         // one problem per DM over all beams: the epilogue resolves each beam's
         // beamset (scale, offset, IB power) itself, so 128-beam tiles pack

@@ -41,8 +41,11 @@ namespace cb {
 constexpr int kM           = 128;  // beams per tile
 constexpr int kTileT       = 64;   // samples per tile
 constexpr int kN           = 2 * kTileT;
-constexpr int kVStages     = 4;
-constexpr int kWStages     = 2;
+// Pipeline depths (copies in flight ahead of the MMAs): runtime choices,
+// voltage stages 2..8 (default 4) and weight stages 2..3 (default 2), picked
+// per shape by sw_autotune.
+constexpr int kVStagesDefault = 4, kVStagesMax = 8;
+constexpr int kWStagesDefault = 2, kWStagesMax = 3;
 constexpr int kTilesPerItem = 64;  // default work item: 4096 samples of one channel
 constexpr int kMaxDm       = 16;
 constexpr int kMaxProblems = 96;
@@ -78,6 +81,7 @@ struct Params {
     int* err;
     uint32_t idesc;
     uint32_t w_layout, w_sbo16, v_lbo16;
+    int vstages, wstages;  // pipeline depths
     unsigned long long timeout_ns;
     int test_stall;  // self-test: the producer issues nothing, so waits run out
 };
@@ -388,14 +392,15 @@ cb_kernel(const __grid_constant__ Params P)
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const int wtile = kM * P.kbytes;              // one A block
     const int vtile = 2 * P.kbytes * kTileT;       // one B stage
-    uint8_t* wbuf = base;                          // [kWStages][2][wtile]
-    uint8_t* vbuf = wbuf + kWStages * 2 * wtile;   // [kVStages][vtile]
-    uint64_t* bars = reinterpret_cast<uint64_t*>(vbuf + kVStages * vtile);
+    const int nvs = P.vstages, nws = P.wstages;
+    uint8_t* wbuf = base;                          // [nws][2][wtile]
+    uint8_t* vbuf = wbuf + nws * 2 * wtile;        // [nvs][vtile]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(vbuf + nvs * vtile);
     uint64_t* v_full    = bars;
-    uint64_t* v_empty   = v_full + kVStages;
-    uint64_t* w_full    = v_empty + kVStages;
-    uint64_t* w_empty   = w_full + kWStages;
-    uint64_t* acc_full  = w_empty + kWStages;
+    uint64_t* v_empty   = v_full + nvs;
+    uint64_t* w_full    = v_empty + nvs;
+    uint64_t* w_empty   = w_full + nws;
+    uint64_t* acc_full  = w_empty + nws;
     uint64_t* acc_empty = acc_full + 2;
     uint64_t* drain     = acc_empty + 2;  // MMA completion on abort
     uint32_t* s_tmem    = reinterpret_cast<uint32_t*>(drain + 1);
@@ -410,8 +415,8 @@ cb_kernel(const __grid_constant__ Params P)
     const unsigned long long deadline = globaltimer() + P.timeout_ns;
 
     if(threadIdx.x == 0) {
-        for(int i = 0; i < kVStages; ++i) { mbar_init(&v_full[i], 1); mbar_init(&v_empty[i], 1); }
-        for(int i = 0; i < kWStages; ++i) { mbar_init(&w_full[i], 1); mbar_init(&w_empty[i], 1); }
+        for(int i = 0; i < nvs; ++i) { mbar_init(&v_full[i], 1); mbar_init(&v_empty[i], 1); }
+        for(int i = 0; i < nws; ++i) { mbar_init(&w_full[i], 1); mbar_init(&w_empty[i], 1); }
         for(int i = 0; i < 2; ++i) { mbar_init(&acc_full[i], 1); mbar_init(&acc_empty[i], kEpiWarps / 2); }
         mbar_init(drain, 1);
         *s_abort = 0;
@@ -448,7 +453,7 @@ cb_kernel(const __grid_constant__ Params P)
                 const uint32_t wdst = wbuf_s + ws * 2 * wtile;
                 tma_load_2d(wdst, &P.wmap, wbar, 0, (it.f * 2 + 0) * P.nbeams + it.b0);
                 tma_load_2d(wdst + wtile, &P.wmap, wbar, 0, (it.f * 2 + 1) * P.nbeams + it.b0);
-                if(++ws == kWStages) { ws = 0; wph ^= 1; }
+                if(++ws == nws) { ws = 0; wph ^= 1; }
                 const int tile0 = it.tc * P.tpi;
                 const int tile1 = min(ntiles_gulp, tile0 + P.tpi);
                 const CUtensorMap* vmap = &P.vmap[pr.dm];
@@ -460,7 +465,7 @@ cb_kernel(const __grid_constant__ Params P)
                     v_armed |= 1u << vs;
                     v_par = (v_par & ~(1u << vs)) | (vph << vs);
                     tma_load_3d(vbuf_s + vs * vtile, vmap, vbar, x, 0, it.f * 2);
-                    if(++vs == kVStages) { vs = 0; vph ^= 1; }
+                    if(++vs == nvs) { vs = 0; vph ^= 1; }
                 }
             }
             // After an abort, let every copy still in flight land before the
@@ -468,10 +473,10 @@ cb_kernel(const __grid_constant__ Params P)
             // bytes arrive; bounded like every other wait).
             if(*s_abort) {
                 const unsigned long long until = globaltimer() + 100ull * 1000 * 1000;
-                for(int i = 0; i < kVStages; ++i)
+                for(int i = 0; i < nvs; ++i)
                     if(v_armed >> i & 1)
                         while(!mbar_try_wait(v_full_s + 8 * i, v_par >> i & 1) && globaltimer() < until) {}
-                for(int i = 0; i < kWStages; ++i)
+                for(int i = 0; i < nws; ++i)
                     if(w_armed >> i & 1)
                         while(!mbar_try_wait(w_full_s + 8 * i, w_par >> i & 1) && globaltimer() < until) {}
             }
@@ -513,11 +518,11 @@ cb_kernel(const __grid_constant__ Params P)
                     // it sees the accumulators (a second commit per tile, for the
                     // stage, measured 2.5 % slower)
                     mma_commit(acc_full_s + 8 * ab);
-                    if(++vs == kVStages) { vs = 0; vph ^= 1; }
+                    if(++vs == nvs) { vs = 0; vph ^= 1; }
                     if(++ab == 2) { ab = 0; aph ^= 1; }
                 }
                 mma_commit(w_empty_s + 8 * ws);
-                if(++ws == kWStages) { ws = 0; wph ^= 1; }
+                if(++ws == nws) { ws = 0; wph ^= 1; }
                 if(!ok) break;
             }
             // After an abort, wait (bounded) for the MMAs already issued, so
@@ -597,7 +602,7 @@ cb_kernel(const __grid_constant__ Params P)
                 if(!mbar_wait(acc_full_s + 8 * grp, aph, s_abort, deadline, P.err)) { ok = false; break; }
                 // the tile's MMAs are complete, so its voltage stage is free
                 if(warp == 2 + 8 * grp && lane == 0)
-                    mbar_arrive(&v_empty[(seq + tile - tile0) % kVStages]);
+                    mbar_arrive(&v_empty[(seq + tile - tile0) % nvs]);
                 fence_after();
                 float power[NC];  // carried across groups while tscrunch > 8
 #pragma unroll
@@ -772,10 +777,10 @@ Params& launch_params()
 
 int dispatch_ts(int ts, int stokes, int grid, size_t smem, cudaStream_t stream);
 
-size_t smem_bytes(int kbytes)
+size_t smem_bytes(int kbytes, int vstages, int wstages)
 {
-    return 1024 + (size_t)kWStages * 2 * kM * kbytes + (size_t)kVStages * 2 * kbytes * kTileT +
-           (2 * kVStages + 2 * kWStages + 5) * 8 + 16;
+    return 1024 + (size_t)wstages * 2 * kM * kbytes + (size_t)vstages * 2 * kbytes * kTileT +
+           (2 * vstages + 2 * wstages + 5) * 8 + 16;
 }
 
 int num_sms()
@@ -811,6 +816,11 @@ int launch(const sw_cb_shape* s, const sw_cb_problem* probs, int nprob,
                "CoherentBeamformer: rows shorter than the gulp");
     SW_REQUIRE(s->nbeams > 0 && s->nchans > 0, "CoherentBeamformer: empty shape");
     SW_REQUIRE(s->row_stride <= 0x7fffffffULL, "CoherentBeamformer: row stride too large");
+    const int vstages = s->voltage_stages > 0 ? s->voltage_stages : kVStagesDefault;
+    const int wstages = s->weight_stages > 0 ? s->weight_stages : kWStagesDefault;
+    SW_REQUIRE(vstages >= 2 && vstages <= kVStagesMax && wstages >= 2 && wstages <= kWStagesMax,
+               "CoherentBeamformer: voltage stages must be 2..%d and weight stages 2..%d",
+               kVStagesMax, kWStagesMax);
 
     Params& P = launch_params();
     memset(&P, 0, sizeof(P));
@@ -878,8 +888,13 @@ int launch(const sw_cb_shape* s, const sw_cb_problem* probs, int nprob,
     P.v_lbo16  = (uint32_t)(2 * s->nantennas * kTileT / 16);          // pol plane stride
     P.timeout_ns = timeout_ns;                                        // 5 s by default
     P.test_stall = test_stall;
+    P.vstages = vstages;
+    P.wstages = wstages;
 
-    const size_t smem = smem_bytes(P.kbytes);
+    const size_t smem = smem_bytes(P.kbytes, P.vstages, P.wstages);
+    SW_REQUIRE(smem <= 227 * 1024,
+               "CoherentBeamformer: %d voltage and %d weight stages need %zu bytes of shared "
+               "memory (at most 232448)", P.vstages, P.wstages, smem);
     const int grid = P.nitems < num_sms() ? P.nitems : num_sms();
     return dispatch_ts(s->tscrunch, s->stokes, grid, smem, stream);
 }

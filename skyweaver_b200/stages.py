@@ -157,10 +157,10 @@ def incoherent_beamform(fpact, nsamples, tscrunch, scale, offset, beamset_weight
 
 
 def cb_shape(fpact, nsamples, nbeams, tscrunch, stokes="I", ib_subtract=True,
-             offset_samples=0, tiles_per_item=0):
+             offset_samples=0, tiles_per_item=0, voltage_stages=0, weight_stages=0):
     F, P, A, _, stride = fpact.shape
     return CbShape(F, nsamples, A, nbeams, tscrunch, STOKES[stokes], int(ib_subtract),
-                   stride, offset_samples, tiles_per_item)
+                   stride, offset_samples, tiles_per_item, voltage_stages, weight_stages)
 
 
 def coherent_beamform(fpact, weights_gemm, scale, offset, mapping, ib_raw, nsamples,
@@ -187,12 +187,13 @@ def coherent_beamform(fpact, weights_gemm, scale, offset, mapping, ib_raw, nsamp
 
 def coherent_beamform_grouped(problems, weights_gemm, scale, offset, mapping, nsamples,
                               tscrunch, stokes="I", ib_subtract=True, offset_samples=0,
-                              tiles_per_item=0, stream=None):
-    """problems: list of (fpact, out, ib_raw, beam_start, beam_count)."""
+                              tiles_per_item=0, voltage_stages=0, weight_stages=0, stream=None):
+    """problems: list of (fpact, out, ib_raw, beam_start, beam_count).
+    voltage_stages / weight_stages: copies in flight (0: library defaults)."""
     fp0 = problems[0][0]
     nbeams = weights_gemm.shape[2]
     shape = cb_shape(fp0, nsamples, nbeams, tscrunch, stokes, ib_subtract, offset_samples,
-                     tiles_per_item)
+                     tiles_per_item, voltage_stages, weight_stages)
     arr = (CbProblem * len(problems))(*[
         CbProblem(p[0].data_ptr(), p[1].data_ptr(), p[2].data_ptr() if p[2] is not None else None,
                   p[3], p[4]) for p in problems])
@@ -294,7 +295,8 @@ def autotune(nantennas, nbeams, nchans, nsamples, tscrunch, dms, centre_frequenc
          ctypes.c_double(centre_frequency), ctypes.c_double(bandwidth), ctypes.byref(t),
          _stream(stream))
     return {"fft_len": t.fft_len, "overlap": t.overlap, "lag": t.lag,
-            "cb_tiles_per_item": t.cb_tiles_per_item,
+            "cb_tiles_per_item": t.cb_tiles_per_item, "cb_voltage_stages": t.cb_voltage_stages,
+            "cb_weight_stages": t.cb_weight_stages,
             "cdd_ms": t.cdd_ms, "cb_ms": t.cb_ms}
 
 

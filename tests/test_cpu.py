@@ -153,6 +153,12 @@ def test_c_abi_rejects_bad_arguments_without_gpu():
     rc = L.sw_coherent_dedisperse_ws(fake, 4096, 1, 2, 4, 2048, 1024, 256, 300, fake, 1, outs,
                                      2048, None, 0, None, None)
     assert rc == 1 and b"lag" in L.sw_last_error()
+    # coherent beamformer pipeline depths outside 2..8 / 2..3
+    shape = _lib.CbShape(1, 64, 16, 128, 4, 0, 1, 64, 0, 0, 9, 2)
+    prob = _lib.CbProblem(0x10000, 0x20000, 0x30000, 0, 128)
+    rc = L.sw_coherent_beamform(ctypes.byref(shape), ctypes.byref(prob), fake, fake, fake, fake,
+                                None, None)
+    assert rc == 1 and b"stages" in L.sw_last_error()
 
 
 def test_output_description_follows_described_vector():

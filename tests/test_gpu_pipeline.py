@@ -275,6 +275,8 @@ def test_autotune_choices_and_results(cuda, oracle):
     t = stages.autotune(A, B, F, T, ts, dms, centre, bw)
     assert t["fft_len"] > t["overlap"] and t["fft_len"] & (t["fft_len"] - 1) == 0
     assert t["cb_tiles_per_item"] in (4, 8, 16, 32, 64, 128)
+    assert (t["cb_voltage_stages"], t["cb_weight_stages"]) in (
+        (4, 2), (2, 2), (3, 2), (6, 2), (8, 2), (4, 3), (6, 3))
     assert t["cdd_ms"] > 0 and t["cb_ms"] > 0
     t0 = time.perf_counter()
     assert stages.autotune(A, B, F, T, ts, dms, centre, bw) == t      # cached

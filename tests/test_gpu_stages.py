@@ -299,6 +299,14 @@ def test_coherent_beam_grouped_equals_plain(cuda, oracle):
     stages.coherent_beamform_grouped(probs, gemm, scales, offs, _dev(cuda, mapping), T, ts)
     for a, b in zip(plain, outs):
         assert np.array_equal(a, _np(b))
+    # every pipeline depth the autotuner may pick gives the same beams
+    for vst, wst in ((2, 2), (3, 2), (6, 2), (8, 2), (4, 3), (6, 3)):
+        for o in outs:
+            o.zero_()
+        stages.coherent_beamform_grouped(probs, gemm, scales, offs, _dev(cuda, mapping), T, ts,
+                                         tiles_per_item=2, voltage_stages=vst, weight_stages=wst)
+        for a, b in zip(plain, outs):
+            assert np.array_equal(a, _np(b)), (vst, wst)
 
 
 # ------------------------------------------------- coherent dedispersion
