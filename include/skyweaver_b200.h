@@ -502,9 +502,8 @@ int sw_pipeline_set_delays(sw_pipeline* p, const float* h_delays,
 int sw_pipeline_process_device(sw_pipeline* p, const void* d_taftp,
                                double epoch, sw_stream_t stream);
 /* Run one gulp from pinned host memory: H2D copy, chain, and D2H of the
- * coherent-beam output of every DM into h_cb_out (may be NULL).  The chain
- * is ordered after the work already queued on `stream`, and `stream` waits
- * for the D2H. */
+ * coherent-beam output of every DM into h_cb_out (may be NULL); `stream`
+ * waits for the D2H. */
 int sw_pipeline_process_host(sw_pipeline* p, const void* h_taftp,
                              double epoch, void* h_cb_out,
                              sw_stream_t stream);
@@ -524,6 +523,10 @@ long sw_pipeline_gulp_count(const sw_pipeline* p);
 int sw_pipeline_gulp_outputs(sw_pipeline* p, long gulp, int dm_idx,
                              const int8_t** d_cb_tfb, const float** d_ib_raw,
                              const int8_t** d_ib_btf, const float** d_stats);
+/* Order the next gulp's chain after the work queued on `stream` so far (e.g.
+ * a handler's copies of the outputs that gulp will overwrite: the outputs
+ * alternate between two buffer sets). */
+int sw_pipeline_order_after(sw_pipeline* p, sw_stream_t stream);
 /* Host wait until the last gulp's pinned input has been copied to the device,
  * after which the caller may reuse that host buffer. */
 int sw_pipeline_wait_input(sw_pipeline* p);

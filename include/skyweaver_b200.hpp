@@ -1420,6 +1420,8 @@ class BeamformerPipeline {
             check(sw_pipeline_set_delays(_p, reinterpret_cast<const float*>(h.data()), _delays.epoch()));
             _uploaded_model = _delays.model_index();
         }
+        // the handlers' work on the gulp this one overwrites comes first
+        check(sw_pipeline_order_after(_p, nullptr));
         if(host) {
             check(sw_pipeline_process_host(_p, data, (double)epoch, nullptr, nullptr));
             check(sw_pipeline_wait_input(_p));

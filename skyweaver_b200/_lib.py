@@ -138,6 +138,7 @@ _SIGS = {
                                          ctypes.POINTER(c_void_p), ctypes.POINTER(c_void_p),
                                          ctypes.POINTER(c_void_p), ctypes.POINTER(c_void_p)]),
     "sw_pipeline_wait_input": (c_int, [c_void_p]),
+    "sw_pipeline_order_after": (c_int, [c_void_p, c_void_p]),
     "sw_pipeline_voltages": (c_int, [c_void_p, c_int, ctypes.POINTER(c_void_p),
                                      ctypes.POINTER(c_size_t)]),
     "sw_pipeline_fft_len": (c_int, [c_void_p, ctypes.POINTER(c_int), ctypes.POINTER(c_int),

@@ -461,10 +461,6 @@ int sw_pipeline_process_host(sw_pipeline* p, const void* h_taftp, double epoch, 
 {
     SW_REQUIRE(p && h_taftp, "sw_pipeline_process_host: null argument");
     const int par = (int)(p->gulp & 1);
-    // the chain runs after the work already on the caller's stream (e.g. a
-    // handler still reading the outputs this parity is about to overwrite)
-    SW_CUDA_CHECK(cudaEventRecord(p->caller_ready[par], as_cuda(stream)));
-    SW_CUDA_CHECK(cudaStreamWaitEvent(p->compute, p->caller_ready[par], 0));
     // H2D into this parity's input buffer once its previous gulp consumed it
     SW_CUDA_CHECK(cudaStreamWaitEvent(p->h2d, p->comp_done[par], 0));
     SW_CUDA_CHECK(cudaMemcpyAsync(p->taftp[par].p, h_taftp, p->taftp[par].n,
@@ -526,6 +522,15 @@ int sw_pipeline_gulp_outputs(sw_pipeline* p, long gulp, int dm_idx, const int8_t
     if(d_ib_raw) *d_ib_raw = p->ib_raw[par][dm_idx].as<float>();
     if(d_ib_btf) *d_ib_btf = p->ib_i8[par][dm_idx].as<int8_t>();
     if(d_stats) *d_stats = p->stats[par].as<float>();
+    return SW_OK;
+}
+
+int sw_pipeline_order_after(sw_pipeline* p, sw_stream_t stream)
+{
+    SW_REQUIRE(p, "sw_pipeline_order_after: null pipeline");
+    const int par = (int)(p->gulp & 1);
+    SW_CUDA_CHECK(cudaEventRecord(p->caller_ready[par], as_cuda(stream)));
+    SW_CUDA_CHECK(cudaStreamWaitEvent(p->compute, p->caller_ready[par], 0));
     return SW_OK;
 }
 
