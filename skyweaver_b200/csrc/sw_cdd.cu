@@ -535,440 +535,6 @@ cdd_kernel(const __grid_constant__ Args A)
     asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
-// --------------------------------------- paired-butterfly transform (N >= 2048)
-// The same mixed-radix DIF forward / DIT inverse as cdd_kernel, with two
-// butterflies per thread (N / 32 threads): butterfly b and its partner
-// b + N/(2R) ride in the two lanes of packed f32x2 registers, so every
-// butterfly operation (add, subtract, multiply, fused multiply-add) is one
-// instruction for two butterflies.  Shared memory holds the window planar
-// (a float plane of real parts and one of imaginary parts) so that a lane
-// loads or stores its own float.  In the radix-16 passes the partners share
-// their twiddles (they lie N/2 apart), which are loaded once per pair.  The
-// chirp table holds, per thread and spectral register, the chirps of both
-// lanes' bins as {cos A, cos B, sin A, sin B}.
-__device__ __forceinline__ uint64_t pk(float a, float b)
-{
-    uint64_t r;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
-    return r;
-}
-__device__ __forceinline__ float lane_a(uint64_t v)
-{
-    float a;
-    asm("mov.b64 {%0, _}, %1;" : "=f"(a) : "l"(v));
-    return a;
-}
-__device__ __forceinline__ float lane_b(uint64_t v)
-{
-    float b;
-    asm("mov.b64 {_, %0}, %1;" : "=f"(b) : "l"(v));
-    return b;
-}
-__device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b)
-{
-    uint64_t d;
-    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-}
-__device__ __forceinline__ uint64_t sub2(uint64_t a, uint64_t b)
-{
-    uint64_t d;
-    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-}
-__device__ __forceinline__ uint64_t mul2(uint64_t a, uint64_t b)
-{
-    uint64_t d;
-    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-}
-__device__ __forceinline__ uint64_t fma2(uint64_t a, uint64_t b, uint64_t c)
-{
-    uint64_t d;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
-    return d;
-}
-
-// two complex values, one per lane
-struct cp {
-    uint64_t re, im;
-};
-__device__ __forceinline__ cp padd(cp a, cp b) { return {add2(a.re, b.re), add2(a.im, b.im)}; }
-__device__ __forceinline__ cp psub(cp a, cp b) { return {sub2(a.re, b.re), sub2(a.im, b.im)}; }
-// a * w for lane twiddles w = c + i s (ns = -s): one rounded product, one fma
-__device__ __forceinline__ cp pmul(cp a, uint64_t c, uint64_t s, uint64_t ns)
-{
-    return {fma2(a.re, c, mul2(a.im, ns)), fma2(a.re, s, mul2(a.im, c))};
-}
-// a * conj(w)
-__device__ __forceinline__ cp pmulc(cp a, uint64_t c, uint64_t s, uint64_t ns)
-{
-    return {fma2(a.re, c, mul2(a.im, s)), fma2(a.im, c, mul2(a.re, ns))};
-}
-__device__ __forceinline__ uint64_t neg2(uint64_t v) { return mul2(v, pk(-1.0f, -1.0f)); }
-
-// radix 4 with the +-i rotation folded into the adds
-template <bool INV>
-__device__ __forceinline__ void pdft4(cp& x0, cp& x1, cp& x2, cp& x3)
-{
-    const cp t0 = padd(x0, x2), t1 = psub(x0, x2);
-    const cp t2 = padd(x1, x3), d = psub(x1, x3);
-    x0 = padd(t0, t2);
-    x2 = psub(t0, t2);
-    if(!INV) {  // t1 -/+ i d
-        x1 = {add2(t1.re, d.im), sub2(t1.im, d.re)};
-        x3 = {sub2(t1.re, d.im), add2(t1.im, d.re)};
-    } else {
-        x1 = {sub2(t1.re, d.im), add2(t1.im, d.re)};
-        x3 = {add2(t1.re, d.im), sub2(t1.im, d.re)};
-    }
-}
-
-template <bool INV>
-__device__ __forceinline__ void pdft2(cp* x)
-{
-    const cp a = x[0], b = x[1];
-    x[0] = padd(a, b);
-    x[1] = psub(a, b);
-}
-
-// multiply by W16^k (forward sign; conjugate when INV), k in {1,2,3,4,6,9}
-template <bool INV>
-__device__ __forceinline__ cp pw16(cp x, int k)
-{
-    const float c1 = 0.92387953251128675613f, s1 = 0.38268343236508977173f;
-    const float c2 = 0.70710678118654752440f;
-    if(k == 4) {  // -i forward, +i inverse
-        return INV ? cp{neg2(x.im), x.re} : cp{x.im, neg2(x.re)};
-    }
-    float c, s;
-    switch(k) {
-    case 1: c = c1; s = -s1; break;
-    case 2: c = c2; s = -c2; break;
-    case 3: c = s1; s = -c1; break;
-    case 6: c = -c2; s = -c2; break;
-    default: c = -c1; s = s1; break;  // k == 9
-    }
-    if(INV) s = -s;
-    return pmul(x, pk(c, c), pk(s, s), pk(-s, -s));
-}
-
-template <bool INV>
-__device__ __forceinline__ void pdft16(cp* x)
-{
-#pragma unroll
-    for(int r2 = 0; r2 < 4; ++r2) pdft4<INV>(x[r2], x[4 + r2], x[8 + r2], x[12 + r2]);
-#pragma unroll
-    for(int r2 = 1; r2 < 4; ++r2)
-#pragma unroll
-        for(int q1 = 1; q1 < 4; ++q1) x[4 * q1 + r2] = pw16<INV>(x[4 * q1 + r2], r2 * q1);
-#pragma unroll
-    for(int q1 = 0; q1 < 4; ++q1) pdft4<INV>(x[4 * q1], x[4 * q1 + 1], x[4 * q1 + 2], x[4 * q1 + 3]);
-    cp t[16];
-#pragma unroll
-    for(int q1 = 0; q1 < 4; ++q1)
-#pragma unroll
-        for(int q2 = 0; q2 < 4; ++q2) t[q1 + 4 * q2] = x[4 * q1 + q2];
-#pragma unroll
-    for(int i = 0; i < 16; ++i) x[i] = t[i];
-}
-
-template <bool INV>
-__device__ __forceinline__ void pdft8(cp* x)
-{
-#pragma unroll
-    for(int r2 = 0; r2 < 4; ++r2) {
-        const cp a = x[r2], b = x[4 + r2];
-        x[r2]     = padd(a, b);
-        x[4 + r2] = psub(a, b);
-    }
-    const float c2 = 0.70710678118654752440f;
-    const float sg = INV ? c2 : -c2;
-    x[5] = pmul(x[5], pk(c2, c2), pk(sg, sg), pk(-sg, -sg));
-    x[6] = INV ? cp{neg2(x[6].im), x[6].re} : cp{x[6].im, neg2(x[6].re)};
-    x[7] = pmul(x[7], pk(-c2, -c2), pk(sg, sg), pk(-sg, -sg));
-    pdft4<INV>(x[0], x[1], x[2], x[3]);
-    pdft4<INV>(x[4], x[5], x[6], x[7]);
-    cp t[8];
-#pragma unroll
-    for(int q2 = 0; q2 < 4; ++q2) {
-        t[2 * q2]     = x[q2];
-        t[2 * q2 + 1] = x[4 + q2];
-    }
-#pragma unroll
-    for(int i = 0; i < 8; ++i) x[i] = t[i];
-}
-
-template <int R, bool INV>
-__device__ __forceinline__ void pdft(cp* x)
-{
-    if constexpr(R == 16) pdft16<INV>(x);
-    else if constexpr(R == 8) pdft8<INV>(x);
-    else if constexpr(R == 4) pdft4<INV>(x[0], x[1], x[2], x[3]);
-    else pdft2<INV>(x);
-}
-
-// planar shared memory: lane A's value at re[ia], lane B's at re[ib]
-__device__ __forceinline__ cp pload(const float* re, const float* im, int ia, int ib)
-{
-    return {pk(re[ia], re[ib]), pk(im[ia], im[ib])};
-}
-__device__ __forceinline__ void pstore(float* re, float* im, int ia, int ib, cp v)
-{
-    re[ia] = lane_a(v.re);
-    re[ib] = lane_b(v.re);
-    im[ia] = lane_a(v.im);
-    im[ib] = lane_b(v.im);
-}
-
-// twiddles w_q = W_G^(j q), q = 1..R-1, of column j as lane pairs: the same
-// j for both lanes (ja == jb) or one each
-template <int R>
-__device__ __forceinline__ void load_tw2(const c32* tw_s, int tw_off, int s, int ja, int jb,
-                                         uint64_t* c, uint64_t* sn, uint64_t* ns)
-{
-    c32 wa[R], wb[R];
-    load_tw<R>(tw_s, tw_off, s, ja, wa);
-    if(jb == ja) {
-#pragma unroll
-        for(int q = 1; q < R; ++q) wb[q] = wa[q];
-    } else {
-        load_tw<R>(tw_s, tw_off, s, jb, wb);
-    }
-#pragma unroll
-    for(int q = 1; q < R; ++q) {
-        c[q]  = pk(wa[q].x, wb[q].x);
-        sn[q] = pk(wa[q].y, wb[q].y);
-        ns[q] = pk(-wa[q].y, -wb[q].y);
-    }
-}
-
-// Twiddle w = (c, s) shared by both lanes of a pair; forward or conjugate.
-template <bool CONJ>
-__device__ __forceinline__ cp ptw(cp x, float c, float s)
-{
-    return CONJ ? pmulc(x, pk(c, c), pk(s, s), pk(-s, -s)) : pmul(x, pk(c, c), pk(s, s), pk(-s, -s));
-}
-
-// One radix-16 pass (stride s, span G) over both lanes: lane A butterfly
-// tid, lane B tid + N/32 (same column j, N/2 further on), so both lanes use
-// the same twiddles, read as pairs (w_2k+1, w_2k+2) with one 16-byte load
-// and applied as they arrive (few registers while the spectrum is held).
-template <int LOGN, bool FWD>
-__device__ __forceinline__ void ppass16(float* re, float* im, const c32* tw_s, int G, int s,
-                                        int tw_off)
-{
-    constexpr int N = 1 << LOGN;
-    const int beta = threadIdx.x;
-    const int g = beta / s, j = beta - g * s;
-    const int base = g * G + j;
-    const int pa = pad(base);
-    const int db = pad(base + N / 2) - pa;  // lane B offset (constant)
-    cp x[16];
-#pragma unroll
-    for(int r = 0; r < 16; ++r) {
-        const int ia = pad_at(base, pa, r, s);
-        x[r] = pload(re, im, ia, ia + db);
-    }
-    if constexpr(FWD) pdft16<false>(x);
-    if(s > 1) {
-        const float4* tp = reinterpret_cast<const float4*>(tw_s + tw_off);
-#pragma unroll
-        for(int k = 0; k < 8; ++k) {
-            const float4 v = tp[k * s + j];
-            x[2 * k + 1] = ptw<!FWD>(x[2 * k + 1], v.x, v.y);
-            if(k < 7) x[2 * k + 2] = ptw<!FWD>(x[2 * k + 2], v.z, v.w);
-        }
-    }
-    if constexpr(!FWD) pdft16<true>(x);
-#pragma unroll
-    for(int r = 0; r < 16; ++r) {
-        const int ia = pad_at(base, pa, r, s);
-        pstore(re, im, ia, ia + db, x[r]);
-    }
-}
-
-template <int LOGN, bool DBG>
-__global__ void __launch_bounds__((1 << LOGN) / 32, LOGN >= 13 ? 1 : (LOGN == 12 ? 2 : 4))
-cdd2_kernel(const __grid_constant__ Args A)
-{
-    constexpr int N   = 1 << LOGN;
-    constexpr int NT  = N / 32;   // threads: two butterflies (16 points each) per thread
-    constexpr Plan P  = make_plan(LOGN);
-    constexpr int R0  = P.r0;
-    constexpr int B0  = 16 / R0;  // first-pass butterfly pairs per thread
-    constexpr int s0  = N / R0;
-    constexpr int NP  = pad(N) + 16;
-    extern __shared__ __align__(16) uint8_t smem[];
-    float* re  = reinterpret_cast<float*>(smem);
-    float* im  = re + NP;
-    c32* tw_s  = reinterpret_cast<c32*>(im + NP);
-    uint8_t* stage = reinterpret_cast<uint8_t*>(tw_s + ((P.tw_total + 1) & ~1));
-    for(int i = threadIdx.x; i < P.tw_total; i += NT) tw_s[i] = A.tw[i];
-
-    const int L = N - A.overlap;
-    const int head = A.overlap - A.lag;  // trimmed at the start of each window
-    const uint64_t inv_n = pk(1.0f / (float)N, 1.0f / (float)N);  // exact (power of two)
-    const int nitems = A.nstreams * A.nseg;
-    const bool aligned = (A.row_stride % 16 == 0) && (L % 16 == 0) &&
-                         ((reinterpret_cast<uintptr_t>(A.in) & 15) == 0);
-    uint32_t zero_dms = 0;
-    if constexpr(!DBG)
-        for(int d = 0; d < A.ndms && d < 32; ++d) zero_dms |= (A.zero_flags[d] ? 1u : 0u) << d;
-    const bool copy16 = aligned && (head % 16) == 0 && (A.out_stride % 16) == 0;
-    if(blockIdx.x < nitems) stage_input<N, NT>(stage, A, blockIdx.x, L, aligned);
-    for(int item = blockIdx.x; item < nitems; item += gridDim.x) {
-        const int stream = item / A.nseg;
-        const int seg    = item - stream * A.nseg;
-        const int f      = stream / A.npa;
-        const int start  = seg * L;  // first input sample of the window
-        asm volatile("cp.async.wait_all;" ::: "memory");
-        __syncthreads();
-
-        // ---- forward pass 0 (radix R0, span N) from the staged int8 window:
-        // lane A column j, lane B column j + s0 / 2
-#pragma unroll
-        for(int u = 0; u < B0; ++u) {
-            const int ja = threadIdx.x + u * NT, jb = ja + s0 / 2;
-            cp x[R0];
-#pragma unroll
-            for(int r = 0; r < R0; ++r) {
-                const int ia = ja + r * s0, ib = jb + r * s0;
-                x[r] = {pk((float)(int8_t)stage[ia], (float)(int8_t)stage[ib]),
-                        pk((float)(int8_t)stage[N + ia], (float)(int8_t)stage[N + ib])};
-            }
-            pdft<R0, false>(x);
-            {
-                uint64_t c[R0], sn[R0], ns[R0];
-                load_tw2<R0>(tw_s, P.tw_off[0], s0, ja, jb, c, sn, ns);
-#pragma unroll
-                for(int q = 1; q < R0; ++q) x[q] = pmul(x[q], c[q], sn[q], ns[q]);
-            }
-#pragma unroll
-            for(int q = 0; q < R0; ++q)
-                pstore(re, im, pad_at(ja, pad(ja), q, s0), pad_at(jb, pad(jb), q, s0), x[q]);
-        }
-        for(uint32_t zm = zero_dms; zm; zm &= zm - 1) {
-            const int d = __ffs(zm) - 1;
-            uint8_t* o_re = A.out[d] + (size_t)stream * 2 * A.out_stride;
-            const int n = min(L, A.nsamples - start);  // kept samples of this window
-            if(copy16 && ((reinterpret_cast<uintptr_t>(A.out[d]) & 15) == 0)) {
-                const int chunks = (n + 15) / 16;
-                for(int c = threadIdx.x; c < 2 * chunks; c += NT) {
-                    const int plane = c >= chunks;
-                    const int k = (c - plane * chunks) * 16;
-                    const uint8_t* src = stage + plane * N + head + k;
-                    uint8_t* dst = o_re + plane * A.out_stride + start + k;
-                    if(k + 16 <= n) {
-                        *reinterpret_cast<uint4*>(dst) = *reinterpret_cast<const uint4*>(src);
-                    } else {
-                        for(int b = 0; b < n - k; ++b) dst[b] = src[b];
-                    }
-                }
-            } else {
-                for(int i = threadIdx.x; i < 2 * n; i += NT) {
-                    const int plane = i >= n, k = i - plane * n;
-                    o_re[plane * A.out_stride + start + k] = stage[plane * N + head + k];
-                }
-            }
-        }
-        __syncthreads();
-        if(item + (int)gridDim.x < nitems)
-            stage_input<N, NT>(stage, A, item + gridDim.x, L, aligned);
-        // ---- forward radix-16 passes except the last
-#pragma unroll
-        for(int p = 1; p < P.npass - 1; ++p) {
-            ppass16<LOGN, true>(re, im, tw_s, P.span[p], P.stride[p], P.tw_off[p]);
-            __syncthreads();
-        }
-        // ---- last forward pass (span 16): spectrum -> registers
-        cp spec[16];
-        {
-            const int pa = pad(threadIdx.x * 16), pb = pad(threadIdx.x * 16 + N / 2);
-#pragma unroll
-            for(int r = 0; r < 16; ++r) spec[r] = pload(re, im, pa + r, pb + r);
-        }
-        pdft16<false>(spec);
-
-        // chirp of register r: float4 {cos A, cos B, sin A, sin B} at [r][tid]
-        const float4* chp = reinterpret_cast<const float4*>(A.chirp + (size_t)f * N) + threadIdx.x;
-        const size_t chirp_stride4 = A.chirp_dm_stride / 2;  // float4 per DM
-        int d = 0;
-        while(d < A.ndms && d < 32 && ((zero_dms >> d) & 1u)) ++d;
-        float4 chn[16];
-        if(d < A.ndms) {
-#pragma unroll
-            for(int r = 0; r < 16; ++r) chn[r] = chp[(size_t)d * chirp_stride4 + r * NT];
-        }
-        __syncthreads();
-        for(; d < A.ndms;) {
-            int dn = d + 1;
-            while(dn < A.ndms && dn < 32 && ((zero_dms >> dn) & 1u)) ++dn;
-            cp y[16];
-#pragma unroll
-            for(int r = 0; r < 16; ++r) {
-                const uint64_t c = pk(chn[r].x, chn[r].y), s = pk(chn[r].z, chn[r].w);
-                y[r] = pmul(spec[r], c, s, neg2(s));
-            }
-            if(dn < A.ndms) {  // next DM's chirp, in flight during this inverse
-#pragma unroll
-                for(int r = 0; r < 16; ++r) chn[r] = chp[(size_t)dn * chirp_stride4 + r * NT];
-            }
-            pdft16<true>(y);
-            {
-                const int pa = pad(threadIdx.x * 16), pb = pad(threadIdx.x * 16 + N / 2);
-#pragma unroll
-                for(int r = 0; r < 16; ++r) pstore(re, im, pa + r, pb + r, y[r]);
-            }
-            __syncthreads();
-#pragma unroll
-            for(int p = P.npass - 2; p >= 1; --p) {
-                ppass16<LOGN, false>(re, im, tw_s, P.span[p], P.stride[p], P.tw_off[p]);
-                __syncthreads();
-            }
-            // ---- inverse pass 0 (radix R0, span N): natural-order output
-            uint8_t* o_re = A.out[d] + (size_t)stream * 2 * A.out_stride;
-            uint8_t* o_im = o_re + A.out_stride;
-#pragma unroll
-            for(int u = 0; u < B0; ++u) {
-                const int ja = threadIdx.x + u * NT, jb = ja + s0 / 2;
-                cp z[R0];
-#pragma unroll
-                for(int q = 0; q < R0; ++q)
-                    z[q] = pload(re, im, pad_at(ja, pad(ja), q, s0), pad_at(jb, pad(jb), q, s0));
-                {
-                    uint64_t c[R0], sn[R0], ns[R0];
-                    load_tw2<R0>(tw_s, P.tw_off[0], s0, ja, jb, c, sn, ns);
-#pragma unroll
-                    for(int q = 1; q < R0; ++q) z[q] = pmulc(z[q], c[q], sn[q], ns[q]);
-                }
-                pdft<R0, true>(z);
-#pragma unroll
-                for(int r = 0; r < R0; ++r) {
-                    const uint64_t zr = mul2(z[r].re, inv_n), zi = mul2(z[r].im, inv_n);
-#pragma unroll
-                    for(int lane = 0; lane < 2; ++lane) {
-                        const int i = (lane ? jb : ja) + r * s0;  // index within the window
-                        const int m = start + i - head;           // output sample in the gulp
-                        if(i >= head && i < head + L && m < A.nsamples) {
-                            const float fr = lane ? lane_b(zr) : lane_a(zr);
-                            const float fi = lane ? lane_b(zi) : lane_a(zi);
-                            o_re[m] = (uint8_t)__float2int_rn(fr);  // int8 wrap
-                            o_im[m] = (uint8_t)__float2int_rn(fi);
-                            if constexpr(DBG)
-                                A.dbg[((size_t)d * A.nstreams + stream) * A.nsamples + m] =
-                                    make_float2(fr, fi);
-                        }
-                    }
-                }
-            }
-            __syncthreads();
-            d = dn;
-        }
-    }
-    asm volatile("cp.async.wait_all;" ::: "memory");
-}
-
 // ------------------------------------------------- long FFTs (N = S x 8192)
 // Overlap-save windows longer than one CTA's shared memory are split four-step
 // style into S = N / 8192 sub-transforms of M = 8192 points:
@@ -1249,33 +815,6 @@ __global__ void chirp_k(c32* chirp, SetupArgs S)
     }
 }
 
-// Chirp tables of the paired-butterfly kernel: thread t's spectral register r
-// holds bins digit_reverse(16 t + r) (lane A) and digit_reverse(16 t + N/2 + r)
-// (lane B); entry r * (N/32) + t is {cos A, cos B, sin A, sin B}.
-__global__ void chirp2_k(float4* chirp, SetupArgs S)
-{
-    const Plan P = make_plan(S.logn);
-    const int nt = P.n / 32;
-    const size_t per = (size_t)P.n / 2;  // float4 per (DM, channel)
-    const size_t total = (size_t)S.ndms * S.nchans * per;
-    for(size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total;
-        i += (size_t)gridDim.x * blockDim.x) {
-        const int e = (int)(i % per);
-        const int c = (int)((i / per) % S.nchans);
-        const int d = (int)(i / (per * S.nchans));
-        const int r = e / nt, t = e % nt;
-        const double nu0 = S.low_freq + c * S.coarse_bw - 0.5 * S.coarse_bw;
-        double cs[2], sn[2];
-        for(int lane = 0; lane < 2; ++lane) {
-            const int k = digit_reverse(P, 16 * t + lane * (P.n / 2) + r);
-            const double nu = k * S.fine_bw;
-            const double phase = (nu * nu * S.prefactor[d]) / ((nu0 + nu) * nu0 * nu0);
-            sincos(phase, &sn[lane], &cs[lane]);
-        }
-        chirp[i] = make_float4((float)cs[0], (float)cs[1], (float)sn[0], (float)sn[1]);
-    }
-}
-
 // Chirp tables for the split transform: bin k1 + S k2 of sub-transform k1
 // at k1 * M + (the M-point per-thread load order of k2).
 __global__ void chirp_split_k(c32* chirp, SetupArgs S, int split)
@@ -1335,43 +874,12 @@ int launch_logn_dbg(const Args& a, cudaStream_t stream)
     return SW_OK;
 }
 
-template <int LOGN, bool DBG>
-int launch2_logn_dbg(const Args& a, cudaStream_t stream)
-{
-    constexpr int N = 1 << LOGN;
-    constexpr Plan P = make_plan(LOGN);
-    const size_t smem = (size_t)2 * (pad(N) + 16) * sizeof(float) +
-                        (size_t)((P.tw_total + 1) & ~1) * sizeof(c32) + 2 * N;
-    SW_CUDA_CHECK(cudaFuncSetAttribute(cdd2_kernel<LOGN, DBG>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int dev = 0, nsm = 148, per_sm = 1;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    SW_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cdd2_kernel<LOGN, DBG>,
-                                                                 N / 32, smem));
-    if(per_sm < 1) per_sm = 1;
-    const long items = (long)a.nstreams * a.nseg;
-    const long grid  = items < (long)nsm * per_sm ? items : (long)nsm * per_sm;
-    cdd2_kernel<LOGN, DBG><<<(int)grid, N / 32, smem, stream>>>(a);
-    SW_LAUNCH_CHECK();
-    return SW_OK;
-}
-
-// FFT lengths run by the paired-butterfly kernel (the others by cdd_kernel
-// and, above 8192, the split transform)
-constexpr bool paired(int logn) { return logn >= 11 && logn <= 13; }
-
 // the float output for precision studies is a separate instance, so the
 // production kernel carries none of its registers
 template <int LOGN>
 int launch_logn(const Args& a, cudaStream_t stream)
 {
-    if constexpr(paired(LOGN))
-        return a.dbg ? launch2_logn_dbg<LOGN, true>(a, stream)
-                     : launch2_logn_dbg<LOGN, false>(a, stream);
-    else
-        return a.dbg ? launch_logn_dbg<LOGN, true>(a, stream)
-                     : launch_logn_dbg<LOGN, false>(a, stream);
+    return a.dbg ? launch_logn_dbg<LOGN, true>(a, stream) : launch_logn_dbg<LOGN, false>(a, stream);
 }
 
 int log2_exact(int n)
@@ -1534,9 +1042,6 @@ int sw_cdd_chirps(const float* h_dms, int ndms, int nchans, int fft_len,
         SW_LAUNCH_CHECK();
         split_twiddle_k<<<64, 256, 0, as_cuda(stream)>>>(ch + (size_t)ndms * nchans * fft_len,
                                                          split);
-        SW_LAUNCH_CHECK();
-    } else if(paired(logn)) {
-        chirp2_k<<<148 * 4, 256, 0, as_cuda(stream)>>>(reinterpret_cast<float4*>(ch), S);
         SW_LAUNCH_CHECK();
     } else {
         chirp_k<<<148 * 4, 256, 0, as_cuda(stream)>>>(ch, S);

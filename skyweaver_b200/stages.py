@@ -458,17 +458,21 @@ class BeamformerPipeline:
         shape = (T, self.nchans, self.nbeams) + ((4,) if self.stokes == "IQUV" else ())
         return _device_view(pcb.value, int(np.prod(shape))).view(torch.int8).reshape(shape)
 
-    def voltages(self, dm_idx: int):
+    def voltages(self, dm_idx: int, channels=None):
         """A copy of the last gulp's voltages that fed the beamformers for one
         DM, as FPACT int8 [F][P][A][re|im][gulp] (dedispersed and delayed by the
-        plan's lag, or as transposed without coherent dedispersion)."""
+        plan's lag, or as transposed without coherent dedispersion); only the
+        given channels when `channels` is a list."""
         p, stride = ctypes.c_void_p(), ctypes.c_size_t()
         call("sw_pipeline_voltages", self.h, dm_idx, ctypes.byref(p), ctypes.byref(stride))
         torch.cuda.synchronize()
         rows = self.nchans * 2 * self._nant * 2
         v = _device_view(p.value, (rows - 1) * stride.value + self.gulp).view(torch.int8)
-        return v.as_strided((rows, self.gulp), (stride.value, 1)).cpu().numpy().reshape(
-            self.nchans, 2, self._nant, 2, self.gulp)
+        v = v.as_strided((self.nchans, 4 * self._nant, self.gulp), (4 * self._nant * stride.value,
+                                                                     stride.value, 1))
+        if channels is not None:
+            v = v[list(channels)]
+        return v.cpu().numpy().reshape(v.shape[0], 2, self._nant, 2, self.gulp)
 
     def cb_bytes_per_dm(self):
         return lib().sw_pipeline_cb_bytes_per_dm(self.h)
