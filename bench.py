@@ -337,8 +337,13 @@ def main_b200(args):
                   beamset_weights=bwts, beamset_mapping=mapping)
     # the autotuner picks the FFT length, the beamformer's work-item size and
     # its pipeline depths for this shape (cached for the process)
-    tune = stages.autotune(A, B, F, T, ts, dms, centre, bwidth)
-    pipe = stages.BeamformerPipeline(**common, grouped=True, use_graph=True, autotune=True)
+    if args.no_autotune:   # the cost model's FFT length and the kernel defaults
+        tune = {"fft_len": 0, "cb_tiles_per_item": 0, "cb_voltage_stages": 0,
+                "cb_weight_stages": 0}
+    else:
+        tune = stages.autotune(A, B, F, T, ts, dms, centre, bwidth)
+    pipe = stages.BeamformerPipeline(**common, grouped=True, use_graph=True,
+                                     autotune=not args.no_autotune)
     pipe.set_delays(delays, 1.7e9)
     fft_len, overlap, lag = pipe.cdd_plan()
     epoch0 = 1.7e9
@@ -371,7 +376,8 @@ def main_b200(args):
     value = rtf * world
 
     # ---- plain GPU form: one CB launch per (DM, beamset), no graph
-    plain = stages.BeamformerPipeline(**common, grouped=False, use_graph=False, autotune=True)
+    plain = stages.BeamformerPipeline(**common, grouped=False, use_graph=False,
+                                      autotune=not args.no_autotune)
     plain.set_delays(delays, 1.7e9)
     ms_plain = time_steps(lambda i: plain.process_device(gulp(i), epoch0 + i * gulp_s),
                           max(3, args.steps // 2), 2)
@@ -903,6 +909,9 @@ def main():
     ap.add_argument("--no-uhf", action="store_true",
                     help="skip the UHF beamforming + incoherent dedispersion measurement")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="run the cost model's plan and the kernel defaults instead of "
+                         "the autotuned ones (for profiling captures)")
     args = ap.parse_args()
     if args.profile:
         profile_case(args.profile)
