@@ -43,7 +43,7 @@ WORK = dict(nant=64, nbeams=1024, nchans=64, gulp=65536, tscrunch=16,
 METRIC = "real-time factor & int8 TOPS, 64ant×1024beam×4DM: batched vs plain GPU"
 # dram__bytes_read.sum + dram__bytes_write.sum of one cb_kernel<16,0> launch on
 # the 16-channel, one-DM case of `bench.py --profile cb` (ncu --set full).
-CB_NCU_BYTES_16CH_1DM = 273.018368e6 + 55.531008e6
+CB_NCU_BYTES_16CH_1DM = 273.172736e6 + 55.232512e6
 
 
 def tsamp():
@@ -57,17 +57,18 @@ INPUTS = ("complex Gaussian sigma 8 int8 voltages; narrowband RFI tones at 20 si
           "channels 9, 27 and 45; a DM-100 pulse (64 samples, +3 sigma) in every 20th gulp")
 
 
-def add_rfi_tones(torch, v, channels):
+def add_rfi_tones(torch, v, channels, t0=0):
     """Narrowband RFI: a complex sinusoid of amplitude 160 per component (20
     sigma of the sigma-8 voltages, clipped by the int8 conversion) added to
     every antenna and pol of the given channels of a float TAFTP tensor
-    [heap][antenna][channel][256][pol][re, im]."""
-    t = torch.arange(v.shape[0] * 256, device=v.device, dtype=torch.float32)
+    [heap][antenna][channel][256][pol][re, im] whose first sample is sample
+    `t0` of the stream."""
+    t = torch.arange(v.shape[0] * 256, device=v.device, dtype=torch.float64) + t0
     t = t.reshape(v.shape[0], 256)
     for k, c in enumerate(channels):
-        ph = 2 * math.pi * (0.01 + 0.037 * k) * t
+        ph = torch.remainder((0.01 + 0.037 * k) * t, 1.0) * (2 * math.pi)
         tone = torch.stack([160.0 * torch.cos(ph), 160.0 * torch.sin(ph)], -1)  # [h][s][2]
-        v[:, :, c] += tone[:, None, :, None, :]
+        v[:, :, c] += tone[:, None, :, None, :].to(v.dtype)
 
 
 def workload_gulp(torch, gen, centre, bwidth, pulse, device="cuda"):
@@ -159,6 +160,36 @@ def cpu_baseline(threads=None, nsamp=2048):
             "sample": f"1 of 64 channels x {nsamp} samples, 4 DMs, 1024 beams: "
                       f"{dt:.2f} s on {used} threads, extrapolated x64 channels",
             "seconds": dt}
+
+
+def cpu_baseline_bursts(bursts, threads=None):
+    """The CPU side of C4's burst measurement: the oracle (C restatement of
+    IncoherentDedisperser.cu:66-125, the reference's OpenMP host stage)
+    dedisperses beam 0's coherent beams over each burst's window, and
+    pulse_snr measures the burst on its output exactly as on the GPU's.
+    Adds cpu_snr, cpu_trial and tdb_identical (the GPU's dedispersed window
+    equals the oracle's byte for byte) to every measured burst."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import concurrent.futures as cf
+
+    import swb_oracle as O
+    O.build()
+    tfb0, tdb0 = bursts["_tfb0"], bursts["_tdb0"]
+    dl, maxd, sf = bursts["_delays"], bursts["_maxd"], bursts["_sf"]
+    t0 = time.perf_counter()
+
+    def one(r):
+        if "gpu_snr" not in r:
+            return
+        lo, hi = r["centre"] - 16384, r["centre"] + 16384
+        tdb = O.idd(np.ascontiguousarray(tfb0[lo:hi + maxd, :, None]), dl, maxd, 1, sf)[:, :, 0]
+        snr, j, w, _ = pulse_snr(tdb, 16384)
+        r.update(cpu_snr=round(snr, 3), cpu_trial=j, cpu_boxcar=w,
+                 tdb_identical=bool(np.array_equal(tdb, tdb0[lo:hi])))
+
+    with cf.ThreadPoolExecutor(threads or os.cpu_count() or 1) as ex:
+        list(ex.map(one, bursts["pulses"]))
+    bursts["cpu_seconds"] = round(time.perf_counter() - t0, 2)
 
 
 def run_reference(args):
@@ -466,6 +497,12 @@ def main_b200(args):
             line["uhf"] = {"skipped": f"needs ~120 GB free device memory, {free / 1e9:.0f} GB free"}
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = {k: v for k, v in cpu_baseline().items() if k != "seconds"}
+        if "bursts" in line.get("uhf", {}):
+            cpu_baseline_bursts(line["uhf"]["bursts"])
+    if "bursts" in line.get("uhf", {}):
+        b = line["uhf"]["bursts"]
+        for k in [k for k in b if k.startswith("_")]:
+            del b[k]
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -748,7 +785,118 @@ UHF = dict(nant=64, nchans=256, nbeams=2048, gulp=65536, tscrunch=8, coherent_dm
            idd_dispatch=32768)
 
 
-def uhf_case(torch, stages, synthetic, K, W):
+UHF_STREAM_S = 30.0   # seconds of voltages in the UHF pulse stream
+UHF_NPULSES = 10
+
+
+def pulse_snr(series, centre, guard=2000, half_window=16384):
+    """Recovered S/N of one burst in a dedispersed series float [T][ntrials]
+    (one beam): boxcars of 16..1024 samples (steps of sqrt 2) ending within
+    `guard` samples of `centre`; the noise mean and per-sample standard
+    deviation of each trial come from the samples of [centre - half_window,
+    centre + half_window) farther than `guard` from `centre` (the standard
+    deviation of a W-sample boxcar is taken as sqrt(W) times it: the
+    dedispersed samples are independent).  Returns (S/N, trial index,
+    boxcar width, start sample)."""
+    lo = max(0, centre - half_window)
+    hi = min(series.shape[0], centre + half_window)
+    x = np.asarray(series[lo:hi], np.float64)
+    idx = np.arange(lo, hi)
+    off = np.abs(idx - centre) > guard
+    mu = x[off].mean(axis=0)
+    sd = x[off].std(axis=0)
+    sd[sd == 0] = np.inf
+    cs = np.concatenate([np.zeros((1, x.shape[1])), np.cumsum(x - mu, axis=0)])
+    best = (-np.inf, 0, 0, 0)
+    for k in range(13):
+        w = int(round(16 * 2 ** (k / 2)))
+        s = (cs[w:] - cs[:-w]) / (sd * math.sqrt(w))     # s[i] = boxcar over x[i:i+w]
+        start = np.arange(s.shape[0]) + lo
+        on = np.abs(start + w // 2 - centre) <= guard
+        if not on.any():
+            continue
+        so = s[on]
+        i, j = np.unravel_index(int(np.argmax(so)), so.shape)
+        if so[i, j] > best[0]:
+            best = (float(so[i, j]), int(j), w, int(start[on][i]))
+    return best
+
+
+def uhf_pulse_stream(torch, stages, synthetic, pipe, freqs, trial_dms, trial_delays, maxd, sf,
+                     chbw, lag):
+    """C4's stream: UHF_STREAM_S seconds of fresh sigma-8 voltages with the
+    RFI tones and UHF_NPULSES bursts (DM 250-350, width 1-10 ms, target S/N
+    8-30, at boresight) through the UHF pipeline and the DM-300 block's
+    incoherent dedispersion (trial DMs 250-350).  Beam 0 (boresight) of the
+    coherent beams and of the dedispersed output is kept on the host; the
+    S/N of each burst is measured on the dedispersed output with pulse_snr.
+    Returns the burst list with the recovered S/N and the beam-0 data for
+    the CPU leg."""
+    U = UHF
+    A, F, B, T, ts = U["nant"], U["nchans"], U["nbeams"], U["gulp"], U["tscrunch"]
+    tsamp_raw = 1.0 / chbw
+    ngulps = int(math.ceil(UHF_STREAM_S / (T * tsamp_raw)))
+    g = synthetic.rng(3030)
+    pulses = synthetic.pulse_train(g, UHF_NPULSES, ngulps * T * tsamp_raw)
+    bw = F * chbw
+    low = float(np.float32(U["top"] - bw))
+    inj = synthetic.BurstInjector(torch, pulses, freqs, tsamp_raw, low, bw, A, seed=77)
+    nt = T // ts
+    tfb0 = np.empty((ngulps * nt, F), np.int8)
+    tdb0 = []
+    idp = stages.IncoherentDedispersionPipeline(
+        F, B, [(trial_delays, 1, sf)], lambda b, t: tdb0.append(t[:, :, 0].cpu().numpy()),
+        dispatch=[U["idd_dispatch"]])
+    gen = torch.Generator(device="cuda").manual_seed(8080)
+    taftp = torch.empty((T // 256, A, F, 256, 2, 2), dtype=torch.int8, device="cuda")
+    hc = 32   # heaps per noise chunk (2.1 GB of float noise)
+    for gi in range(ngulps):
+        for h0 in range(0, T // 256, hc):
+            v = torch.empty((hc, A, F, 256, 2, 2), device="cuda").normal_(0.0, 8.0, generator=gen)
+            add_rfi_tones(torch, v, UHF_RFI_CHANNELS, t0=gi * T + h0 * 256)
+            taftp[h0:h0 + hc] = v.round_().clamp_(-127, 127).to(torch.int8)
+            del v
+        inj.inject(taftp, gi * T)
+        pipe.process_device(taftp, 1.7e9 + gi * T * tsamp_raw)
+        cb = pipe.cb_device(1)
+        tfb0[gi * nt:(gi + 1) * nt] = cb[:, :, 0].cpu().numpy()
+        idp.push(0, cb)
+    torch.cuda.synchronize()
+    idp.close()
+    tdb = np.concatenate(tdb0) if tdb0 else np.zeros((0, trial_delays.shape[0]), np.int8)
+    cb_tsamp = ts * tsamp_raw
+    k = synthetic.DM_CONST
+    out = []
+    for p in pulses:
+        # dedispersed sample of the burst: output o sums coherent-beam rows
+        # o + maxd - delay, the burst reaches the top channel at raw sample
+        # t_top / tsamp + lag (the dedisperser's output delay)
+        top = k * p["dm"] * (1 / freqs[0] ** 2 - 1 / freqs[-1] ** 2) / cb_tsamp
+        centre = int(round((p["t_top"] / tsamp_raw + lag) / ts + top - maxd
+                           + 0.5 * p["width"] / cb_tsamp))
+        r = {"t_top_s": round(p["t_top"], 4), "dm": round(p["dm"], 2),
+             "width_ms": round(p["width"] * 1e3, 3), "target_snr": round(p["snr"], 2),
+             "centre": centre}
+        if centre + 16384 > tdb.shape[0]:
+            r["skipped"] = "outside the dispatched output"
+        else:
+            snr, j, w, st = pulse_snr(tdb, centre)
+            # the same trial's float sum of the int8 beams (no division, no
+            # truncation): what the int8 dedispersed output can recover
+            o = np.arange(centre - 16384, centre + 16384)
+            rows = o[:, None] + maxd - trial_delays[j][None, :]
+            flt = tfb0[rows, np.arange(F)[None, :]].astype(np.float64).sum(axis=1)
+            fsnr = pulse_snr(flt[:, None], 16384)[0]
+            r.update(gpu_snr=round(snr, 3), gpu_trial=j,
+                     gpu_trial_dm=round(float(trial_dms[j]), 3), gpu_boxcar=w,
+                     gpu_start=st, beam_float_snr=round(fsnr, 3))
+        out.append(r)
+    return {"stream_s": round(ngulps * T * tsamp_raw, 3), "gulps": ngulps, "beam": 0,
+            "coherent_dm": 300.0, "pulses": out, "_tfb0": tfb0, "_tdb0": tdb,
+            "_delays": trial_delays, "_maxd": maxd, "_sf": sf}
+
+
+def uhf_case(torch, stages, synthetic, K, W, pulses=True):
     """End-to-end UHF chain: 64 antennas x 256 channels (the top of the
     544-1088 MHz band in 1024-channel mode, 0.53125 MHz channels), 2048
     coherent beams + incoherent beam, coherent DMs {0, 300}, tscrunch 8,
@@ -766,6 +914,7 @@ def uhf_case(torch, stages, synthetic, K, W):
     freqs = stages.channel_frequencies(centre, bw, F)
     g = synthetic.rng(1088)
     delays = synthetic.delay_model(g, B, A)
+    delays[0] = [1.0, 0.0, 0.0]   # beam 0 at boresight (the bursts' direction)
     pipe = stages.BeamformerPipeline(nantennas=A, input_nantennas=A, nchans=F, nbeams=B,
                                      gulp_samples=T, tscrunch=ts, centre_frequency=centre,
                                      bandwidth=bw, dms=U["coherent_dms"],
@@ -774,9 +923,10 @@ def uhf_case(torch, stages, synthetic, K, W):
     pipe.set_delays(delays, 1.7e9)
     cb_tsamp = ts / chbw
     k = 4.148806423e15
-    blocks = []
+    blocks, trials_of = [], []
     for dm in U["coherent_dms"]:
         trials = np.abs(np.linspace(dm - U["trial_span"], dm + U["trial_span"], U["ntrials"]))
+        trials_of.append(trials.astype(np.float32))
         dl = np.array([[int(k * (1 / freqs[0] ** 2 - 1 / f ** 2) * d / cb_tsamp + 0.5)
                         for f in freqs] for d in trials.astype(np.float32)], np.int32)
         blocks.append((dl, 1, float(np.float32(math.sqrt(F)))))
@@ -805,18 +955,25 @@ def uhf_case(torch, stages, synthetic, K, W):
     ms = e0.elapsed_time(e1) / K
     geo = [idp.geometry(b) for b in range(len(blocks))]
     idp.close()
-    pipe.close()
     del taftp
     torch.cuda.empty_cache()
     gulp_s = T / chbw
     adds = sum(U["ntrials"] * (T // ts) * B * F for _ in blocks)
-    return {"workload": "UHF 544-1088 MHz (top 256 of 1024 channels), 64 ant x 2048 beams, "
-                        "coherent DMs {0,300}, tscrunch 8, 128 incoherent trials per coherent "
-                        "DM over +-50, device aggregation (dispatch 32768); sigma-8 voltages "
-                        "with RFI tones at 20 sigma in channels 40, 130 and 200",
-            "ms_per_gulp": ms, "rtf": gulp_s / (ms * 1e-3),
-            "idd_adds_per_gulp": adds, "idd_overlap_samples": [g[1] for g in geo],
-            "timed_gulps": K, "warmup_gulps": W}
+    res = {"workload": "UHF 544-1088 MHz (top 256 of 1024 channels), 64 ant x 2048 beams, "
+                       "coherent DMs {0,300}, tscrunch 8, 128 incoherent trials per coherent "
+                       "DM over +-50, device aggregation (dispatch 32768); sigma-8 voltages "
+                       "with RFI tones at 20 sigma in channels 40, 130 and 200",
+           "ms_per_gulp": ms, "rtf": gulp_s / (ms * 1e-3),
+           "idd_adds_per_gulp": adds, "idd_overlap_samples": [g[1] for g in geo],
+           "timed_gulps": K, "warmup_gulps": W}
+    if pulses:
+        _, lag = pipe.cdd_plan()[1:]
+        dl, _, sf = blocks[1]
+        res["bursts"] = uhf_pulse_stream(torch, stages, synthetic, pipe, freqs, trials_of[1],
+                                         dl, int(dl.max()), sf, chbw, lag)
+    pipe.close()
+    torch.cuda.empty_cache()
+    return res
 
 
 def profile_case(which, nchans=16, reps=3):
