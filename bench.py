@@ -108,9 +108,11 @@ def config_block(extra=None):
 # ------------------------------------------------------------ CPU baseline
 def cpu_baseline(threads=None, nsamp=2048):
     """Time the oracle (C restatement of the reference's CPU implementations)
-    on a bounded sample: 1 channel x `nsamp` samples through coherent
-    dedispersion (4 DMs), the incoherent beam and the 1024-beam coherent
-    beamformer; RTF extrapolated linearly to 64 channels."""
+    on a bounded sample: 1 channel x `nsamp` samples of a gulp through every
+    stage of the chain (TAFTP -> FTPA transpose, statistics and scalings,
+    weights of the 1024 beams, coherent dedispersion for 4 DMs, then per DM
+    the incoherent beam and the coherent beamformer); RTF extrapolated
+    linearly to 64 channels (every stage's cost is per channel)."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import concurrent.futures as cf
 
@@ -124,17 +126,24 @@ def cpu_baseline(threads=None, nsamp=2048):
     chbw = WORK["chbw"]
     low = WORK["centre"] - 32 * chbw
     fft_len, ov, lag = O.cdd_plan(WORK["centre"], 64 * chbw, 64, dms)
-    ext = np.clip(np.rint(g.normal(0, 8, size=(1, ov + nsamp, 2, A, 2))), -127, 127).astype(np.int8)
+    taftp = synthetic.voltages_taftp(g, nsamp // 256, A, 1)
+    hist = np.clip(np.rint(g.normal(0, 8, size=(1, ov, 2, A, 2))), -127, 127).astype(np.int8)
     delays = synthetic.delay_model(g, B, A)
     freqs = np.array([low + chbw / 2])
-    w = O.weights(delays, freqs, 0.0, 0.0)
     bw = np.ones((1, A), np.float32)
     mapping = np.zeros(B, np.int32)
-    sc = np.full(1, 1e7, np.float32)
     chirps = {d: O.chirp(1, fft_len, low, chbw, d) for d in dms}
     # tasks: (dm, stream) dedispersion, then (dm, time chunk) beamforming
     nchunk = max(1, min(threads, 16) // len(dms))
+    stage = {}
     t0 = time.perf_counter()
+    ftpa = O.transpose(taftp, A)
+    t1 = time.perf_counter()
+    scl = O.scalings(O.statistics(ftpa), bw, 1, ts, ts, 24.0)
+    t2 = time.perf_counter()
+    w = O.weights(delays, freqs, 0.0, 0.0)
+    t3 = time.perf_counter()
+    ext = np.concatenate([hist, ftpa], axis=1)
     dd = {}
 
     def cdd_task(d):
@@ -143,23 +152,36 @@ def cpu_baseline(threads=None, nsamp=2048):
     with cf.ThreadPoolExecutor(threads) as ex:
         for d, v in ex.map(cdd_task, dms):
             dd[d] = v
+        t4 = time.perf_counter()
 
         def bf_task(args):
             d, c = args
             n = nsamp // nchunk
             x = np.ascontiguousarray(dd[d][:, c * n:(c + 1) * n])
-            raw, _ = O.incoherent_beam(x, ts, sc, sc, bw, 1)
-            return O.coherent_beam(x, w, ts, sc, sc, bw, mapping)
+            O.incoherent_beam(x, ts, scl[3], scl[2], bw, 1)
+            return O.coherent_beam(x, w, ts, scl[1], scl[0], bw, mapping)
 
         list(ex.map(bf_task, [(d, c) for d in dms for c in range(nchunk)]))
-    dt = time.perf_counter() - t0
+    t5 = time.perf_counter()
+    dt = t5 - t0
+    stage = {"transpose": t1 - t0, "statistics_scalings": t2 - t1, "weights": t3 - t2,
+             "coherent_dedispersion": t4 - t3, "beamformers": t5 - t4}
     data_s = nsamp * tsamp()
     rtf = data_s / (dt * WORK["nchans"])
     used = min(threads, len(dms) * nchunk)
     return {"value": rtf, "unit": "x real-time", "cores": used, "kind": "port",
-            "sample": f"1 of 64 channels x {nsamp} samples, 4 DMs, 1024 beams: "
-                      f"{dt:.2f} s on {used} threads, extrapolated x64 channels",
-            "seconds": dt}
+            "sample": f"1 of 64 channels x {nsamp} samples through transpose, statistics, "
+                      f"weights, 4-DM dedispersion and both beamformers (1024 beams): "
+                      f"{dt:.2f} s on up to {used} threads, extrapolated x64 channels",
+            "seconds": dt, "stage_seconds": {k: round(v, 4) for k, v in stage.items()}}
+
+
+def cpu_baseline_median(threads=None, nsamp=2048, runs=3):
+    """cpu_baseline after one untimed warm-up (thread pool, first-touch
+    pages): the run with the median time of `runs`."""
+    cpu_baseline(threads, nsamp=min(nsamp, 1024))
+    vals = sorted((cpu_baseline(threads, nsamp) for _ in range(runs)), key=lambda x: x["seconds"])
+    return vals[len(vals) // 2]
 
 
 def cpu_baseline_bursts(bursts, threads=None):
@@ -499,7 +521,8 @@ def main_b200(args):
         else:
             line["uhf"] = {"skipped": f"needs ~120 GB free device memory, {free / 1e9:.0f} GB free"}
     if rank == 0 and world == 1 and not args.no_cpu:
-        line["cpu_baseline"] = {k: v for k, v in cpu_baseline().items() if k != "seconds"}
+        line["cpu_baseline"] = {k: v for k, v in cpu_baseline_median().items()
+                                if k != "seconds"}
         if "bursts" in line.get("uhf", {}):
             cpu_baseline_bursts(line["uhf"]["bursts"])
     if "bursts" in line.get("uhf", {}):

@@ -139,12 +139,15 @@ def test_incoherent_beam_bit_exact(cuda, oracle, stokes, nbeamsets):
     assert np.array_equal(_np(out), out_ref)
 
 
-@pytest.mark.parametrize("stokes", ["I", "IQUV"])
-def test_incoherent_beam_float_chain_path(cuda, oracle, stokes):
-    """Strong RFI and non-integer weights force the reference-order float chain."""
+@pytest.mark.parametrize("stokes,ts,A", [("I", 32, 64), ("IQUV", 32, 64), ("I", 8, 64),
+                                         ("I", 4, 48), ("I", 16, 80)])
+def test_incoherent_beam_float_chain_path(cuda, oracle, stokes, ts, A):
+    """Strong RFI and non-integer weights force the reference-order float chain:
+    through the 16-sample product table (tscrunch a multiple of 16, at most 64
+    antennas) and byte by byte otherwise."""
     from skyweaver_b200 import stages, synthetic
     g = synthetic.rng(12)
-    A, F, H, ts = 64, 2, 2, 32
+    F, H = 2, 2
     taftp = synthetic.voltages_taftp(g, H, A, F, sigma=8)
     synthetic.inject_tones(taftp, [1], amplitude=110.0)
     ftpa = oracle.transpose(taftp, A)
