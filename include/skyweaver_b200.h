@@ -127,6 +127,20 @@ int sw_statistics(const void* d_fpact, size_t row_stride, size_t sample_offset,
                   int nchans, int npol, int nant, int nsamples,
                   void* d_scratch, float* d_stats, sw_stream_t stream);
 
+/* The TAFTP -> FPACT transpose (sw_transpose_fpact) and the statistics of the
+ * transposed gulp (sw_statistics with npol 2 over its nheaps * 256 samples)
+ * in one pass over the gulp: replaces Transposer::transpose
+ * (cpp/skyweaver/src/Transposer.cu:117-184) followed by
+ * StatisticsCalculator::calculate_statistics
+ * (cpp/skyweaver/src/StatisticsCalculator.cu:54-85,104-130), which read the
+ * voltages twice.  d_fpact and d_stats hold exactly what the two separate
+ * calls write; d_scratch has sw_statistics_scratch_bytes(nchans, 2,
+ * output_nantennas) bytes. */
+int sw_transpose_fpact_statistics(const void* d_taftp, void* d_fpact, int nheaps,
+                                  int input_nantennas, int output_nantennas, int nchans,
+                                  size_t row_stride, size_t sample_offset, void* d_scratch,
+                                  float* d_stats, sw_stream_t stream);
+
 /* No counterpart in the reference.  Same result as sw_statistics, for callers
  * that cannot allocate device memory (a real-time ingest loop that must not
  * take cudaMalloc's implicit device synchronisation, or a process whose

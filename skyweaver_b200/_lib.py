@@ -78,6 +78,9 @@ _SIGS = {
     "sw_statistics_scratch_bytes": (c_size_t, [c_int, c_int, c_int]),
     "sw_statistics": (c_int, [c_void_p, c_size_t, c_size_t, c_int, c_int, c_int, c_int,
                               c_void_p, c_void_p, c_void_p]),
+    "sw_transpose_fpact_statistics": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int,
+                                              c_size_t, c_size_t, c_void_p, c_void_p,
+                                              c_void_p]),
     "sw_statistics_noalloc": (c_int, [c_void_p, c_size_t, c_size_t, c_int, c_int, c_int, c_int,
                                       c_void_p, c_void_p]),
     "sw_update_scalings": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int,

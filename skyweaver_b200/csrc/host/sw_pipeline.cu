@@ -275,10 +275,10 @@ int sw_pipeline::enqueue_chain(const void* d_in, int parity, bool first)
     if(overlap > 0)
         SW_TRY(sw_fpact_copy_history(ext[parity ^ 1].p, rows, nrows, ext_stride,
                                      (size_t)overlap, ss));
-    SW_TRY(sw_transpose_fpact(d_in, rows, nheaps, cfg.input_nantennas, A, F, ext_stride,
-                              ext_off, ss));
-    SW_TRY(sw_statistics(rows, ext_stride, ext_off, F, 2, A, T, stats_scratch.p,
-                         stats[parity].as<float>(), ss));
+    // transpose and statistics in one pass over the gulp
+    SW_TRY(sw_transpose_fpact_statistics(d_in, rows, nheaps, cfg.input_nantennas, A, F,
+                                         ext_stride, ext_off, stats_scratch.p,
+                                         stats[parity].as<float>(), ss));
     const int* chan_order = nullptr;
     if(ib_order.p) {
         SW_TRY(swb::launch_ib_channel_order(stats[parity].as<float>(), F, 2, A,

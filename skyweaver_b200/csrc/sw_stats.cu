@@ -88,6 +88,86 @@ stats_partial_k(const uint8_t* __restrict__ fpact, size_t row_stride,
     }
 }
 
+// TAFTP -> FPACT transpose with the statistics of the same pass: the
+// transpose of sw_layout.cu (16 input bytes = 4 samples x 2 pols x re/im of
+// one antenna -> one 32-bit word in each of the four planar rows) plus the
+// exact S1..S4 sums of those words, so the gulp is read once for both.  A
+// CTA is (hpc heaps, one channel); its 256 threads take 4 antennas x
+// 64 16-byte chunks of a heap, walk the CTA's heaps for each antenna group
+// and add one warp-reduced set of sums per (antenna, pol) into the int64
+// workspace (the two warps of an antenna both add).  Padded antennas (a >=
+// in_nant) are written as zeros and summed as zeros, like the separate
+// stages.  The sums cost more issue than the copy, so the kernel is
+// issue-bound: on a 64 ant x 64 ch x 65536-sample gulp (with its memset) 16,
+// 8, 4, 2 and 1 heaps per CTA took 0.542, 0.498, 0.526, 0.633 and 1.042 ms,
+// against 0.342 + 0.278 ms for the separate transpose and statistics (16
+// heaps leave a second wave of CTAs that fills a third of the SMs).
+constexpr int kFuseHeaps = 8;
+constexpr int kHeapSamples = 256;
+
+__device__ __forceinline__ uint32_t bperm(uint32_t a, uint32_t b, uint32_t sel)
+{
+    return __byte_perm(a, b, sel);
+}
+
+__global__ void __launch_bounds__(256)
+transpose_stats_k(const uint4* __restrict__ taftp, uint8_t* __restrict__ fpact,
+                  int in_nant, int out_nant, int nchans, int nheaps, size_t row_stride,
+                  size_t sample_offset, unsigned long long* __restrict__ sums, int hpc)
+{
+    const int f  = blockIdx.y;
+    const int h0 = blockIdx.x * hpc;
+    const int h1 = min(nheaps, h0 + hpc);
+    const int c = threadIdx.x & 63, lane = threadIdx.x & 31;
+    for(int ag = 0; ag < out_nant; ag += 4) {
+        const int a = ag + (int)(threadIdx.x >> 6);  // uniform across a warp
+        int s1[2] = {0, 0}, s2[2] = {0, 0};
+        long long s3[2] = {0, 0}, s4[2] = {0, 0};
+        if(a < out_nant) {
+            const size_t base0 = (((size_t)f * 2 + 0) * out_nant + a) * 2 * row_stride + sample_offset;
+            const size_t base1 = (((size_t)f * 2 + 1) * out_nant + a) * 2 * row_stride + sample_offset;
+            for(int h = h0; h < h1; ++h) {
+                uint32_t r0 = 0, r1 = 0, r2 = 0, r3 = 0;
+                if(a < in_nant) {
+                    const uint4 v = taftp[(((size_t)h * in_nant + a) * nchans + f) * 64 + c];
+                    const uint32_t t0 = bperm(v.x, v.y, 0x5140), t1 = bperm(v.z, v.w, 0x5140);
+                    const uint32_t t2 = bperm(v.x, v.y, 0x7362), t3 = bperm(v.z, v.w, 0x7362);
+                    r0 = bperm(t0, t1, 0x5410);  // p0 re
+                    r1 = bperm(t0, t1, 0x7632);  // p0 im
+                    r2 = bperm(t2, t3, 0x5410);  // p1 re
+                    r3 = bperm(t2, t3, 0x7632);  // p1 im
+                }
+                const size_t s = (size_t)h * kHeapSamples + c * 4;
+                *reinterpret_cast<uint32_t*>(fpact + base0 + s)              = r0;
+                *reinterpret_cast<uint32_t*>(fpact + base0 + row_stride + s) = r1;
+                *reinterpret_cast<uint32_t*>(fpact + base1 + s)              = r2;
+                *reinterpret_cast<uint32_t*>(fpact + base1 + row_stride + s) = r3;
+                int s3w = 0;  // 8 cubes per pol: |sum| <= 2^24
+                accum_word(r0, s1[0], s2[0], s3w, s4[0]);
+                accum_word(r1, s1[0], s2[0], s3w, s4[0]);
+                s3[0] += s3w;
+                s3w = 0;
+                accum_word(r2, s1[1], s2[1], s3w, s4[1]);
+                accum_word(r3, s1[1], s2[1], s3w, s4[1]);
+                s3[1] += s3w;
+            }
+        }
+        long long v[8] = {s1[0], s2[0], s3[0], s4[0], s1[1], s2[1], s3[1], s4[1]};
+#pragma unroll
+        for(int o = 16; o > 0; o >>= 1)
+#pragma unroll
+            for(int k = 0; k < 8; ++k) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+        if(lane == 0 && a < out_nant) {
+#pragma unroll
+            for(int p = 0; p < 2; ++p)
+#pragma unroll
+                for(int k = 0; k < 4; ++k)
+                    atomicAdd(&sums[(((size_t)f * 2 + p) * out_nant + a) * 4 + k],
+                              (unsigned long long)v[4 * p + k]);
+        }
+    }
+}
+
 __global__ void stats_finalize_k(const long long* __restrict__ sums,
                                  float4* __restrict__ stats, int nseries,
                                  int nsamples)
@@ -234,6 +314,40 @@ int sw_statistics_noalloc(const void* d_fpact, size_t row_stride, size_t sample_
     // launch_statistics clears the sums before accumulating into them
     return launch_statistics(d_fpact, row_stride, sample_offset, nchans, npol, nant, nsamples,
                              sums, d_stats, as_cuda(stream));
+}
+
+int sw_transpose_fpact_statistics(const void* d_taftp, void* d_fpact, int nheaps,
+                                  int input_nantennas, int output_nantennas, int nchans,
+                                  size_t row_stride, size_t sample_offset, void* d_scratch,
+                                  float* d_stats, sw_stream_t stream)
+{
+    SW_REQUIRE(d_taftp && d_fpact && d_scratch && d_stats,
+               "sw_transpose_fpact_statistics: null pointer");
+    SW_REQUIRE(nheaps > 0 && nchans > 0, "sw_transpose_fpact_statistics: empty input");
+    SW_REQUIRE(input_nantennas > 0 && input_nantennas <= output_nantennas,
+               "Input number of antennas must be <= to the maximum nantennas");
+    SW_REQUIRE(row_stride % 16 == 0 && sample_offset % 16 == 0,
+               "sw_transpose_fpact_statistics: row stride and offset must be multiples of 16");
+    SW_REQUIRE(sample_offset + (size_t)nheaps * kHeapSamples <= row_stride,
+               "sw_transpose_fpact_statistics: rows too short for the gulp");
+    SW_REQUIRE(nchans <= 65535, "sw_transpose_fpact_statistics: too many channels");
+    const int nseries = nchans * 2 * output_nantennas;
+    const size_t sum_bytes = (size_t)nseries * 4 * sizeof(long long);
+    cudaStream_t s = as_cuda(stream);
+    SW_CUDA_CHECK(cudaMemsetAsync(d_scratch, 0, sum_bytes, s));
+    dim3 grid(cdiv(nheaps, kFuseHeaps), nchans);
+    transpose_stats_k<<<grid, 256, 0, s>>>(static_cast<const uint4*>(d_taftp),
+                                          static_cast<uint8_t*>(d_fpact), input_nantennas,
+                                          output_nantennas, nchans, nheaps, row_stride,
+                                          sample_offset,
+                                          static_cast<unsigned long long*>(d_scratch),
+                                          kFuseHeaps);
+    SW_LAUNCH_CHECK();
+    stats_finalize_k<<<cdiv(nseries, 256), 256, 0, s>>>(
+        static_cast<const long long*>(d_scratch), reinterpret_cast<float4*>(d_stats), nseries,
+        nheaps * kHeapSamples);
+    SW_LAUNCH_CHECK();
+    return SW_OK;
 }
 
 size_t sw_statistics_scratch_bytes(int nchans, int npol, int nant)

@@ -109,6 +109,24 @@ def statistics(fpact, nsamples, offset=0, stream=None):
     return stats
 
 
+def transpose_fpact_statistics(taftp, out_nant, row_stride=None, offset=0, out=None,
+                               stream=None):
+    """The TAFTP -> FPACT transpose and the statistics of the gulp in one pass
+    over the voltages: (fpact, float [F][2][out_nant][4]), equal to
+    transpose_fpact followed by statistics."""
+    H, A_in, F = taftp.shape[:3]
+    T = H * 256
+    row_stride = row_stride or (offset + T)
+    if out is None:
+        out = torch.zeros((F, 2, out_nant, 2, row_stride), dtype=torch.int8, device=taftp.device)
+    scratch = torch.empty(lib().sw_statistics_scratch_bytes(F, 2, out_nant), dtype=torch.uint8,
+                          device=taftp.device)
+    stats = torch.empty((F, 2, out_nant, 4), dtype=torch.float32, device=taftp.device)
+    call("sw_transpose_fpact_statistics", _ptr(taftp), _ptr(out), H, A_in, out_nant, F,
+         row_stride, offset, _ptr(scratch), _ptr(stats), _stream(stream))
+    return out, stats
+
+
 def update_scalings(stats, beamset_weights, cb_tscrunch, ib_tscrunch, output_level,
                     stream=None):
     """StatisticsCalculator::update_scalings -> (cb_off, cb_scl, ib_off, ib_scl)."""

@@ -75,6 +75,28 @@ def test_statistics(cuda, oracle):
     np.testing.assert_allclose(got, ref, rtol=1e-5, atol=1e-6)
 
 
+@pytest.mark.parametrize("nheaps,in_nant,out_nant", [(8, 64, 64), (20, 57, 64), (3, 12, 16)])
+def test_transpose_statistics_fused_equals_separate(cuda, oracle, nheaps, in_nant, out_nant):
+    """The one-pass transpose + statistics writes the same FPACT bytes and the
+    same statistics (bit for bit) as the two separate stages, padded
+    antennas and a heap count that is not a multiple of the CTA's 16 heaps
+    included; the statistics match the oracle within its tolerance."""
+    from skyweaver_b200 import stages, synthetic
+    g = synthetic.rng(4242)
+    taftp = _dev(cuda, synthetic.voltages_taftp(g, nheaps, in_nant, 5, sigma=20))
+    T, off = nheaps * 256, 80
+    fp0 = stages.transpose_fpact(taftp, out_nant, row_stride=T + off + 16, offset=off)
+    st0 = stages.statistics(fp0, T, offset=off)
+    fp1, st1 = stages.transpose_fpact_statistics(taftp, out_nant, row_stride=T + off + 16,
+                                                 offset=off)
+    assert cuda.equal(fp0, fp1)
+    a, b = _np(st0), _np(st1)
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    ref = oracle.statistics(oracle.transpose(_np(taftp), out_nant))
+    valid = np.arange(out_nant) < in_nant
+    np.testing.assert_allclose(b[:, :, valid], ref[:, :, valid], rtol=1e-5, atol=1e-6)
+
+
 def test_scalings_bit_exact(cuda, oracle):
     from skyweaver_b200 import stages, synthetic
     g = synthetic.rng(5)
