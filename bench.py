@@ -518,7 +518,9 @@ def main_b200(args):
     if not args.no_uhf:
         free, _ = torch.cuda.mem_get_info()
         if free >= 120e9:   # the UHF chain holds ~100 GB (aggregation buffers included)
-            line["uhf"] = uhf_case(torch, stages, synthetic, max(8, (args.steps + 3) // 4 * 4), 8)
+            # the burst stream (C4's S/N measurement) runs on one GPU only
+            line["uhf"] = uhf_case(torch, stages, synthetic, max(8, (args.steps + 3) // 4 * 4), 8,
+                                   pulses=(world == 1))
         else:
             line["uhf"] = {"skipped": f"needs ~120 GB free device memory, {free / 1e9:.0f} GB free"}
     if rank == 0 and world == 1 and not args.no_cpu:
