@@ -477,7 +477,7 @@ def main_b200(args):
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
     cb = kern["coherent_beamformer"]
     # DRAM bytes of one cb_kernel launch from the ncu capture of the 16-channel,
-    # one-DM profile case (dram__bytes_read.sum 273.0 MB + write 55.5 MB),
+    # one-DM profile case (dram__bytes_read.sum 273.2 MB + write 55.2 MB),
     # scaled by the channels x DMs one grouped launch processes.
     traffic = CB_NCU_BYTES_16CH_1DM * (F / 16.0) * len(dms)
     algo_bytes = len(dms) * (F * 2 * A * 2 * T + (T // WORK["tscrunch"]) * F * B)
@@ -488,6 +488,23 @@ def main_b200(args):
             "algorithmic_bytes": algo_bytes,
             "peak_source": "2x measured bf16 cuBLAS burst (MEASURED_PEAKS.json)"
             if peaks else "2x fallback bf16 1.59 PFLOP/s"}
+    # the other stages against their own bounds: HBM (measured copy) for the
+    # byte-moving stages, the CUDA cores' FP32 rate for the FFT dedisperser
+    # (148 SMs x 128 lanes x 2 flop at the timed region's median SM clock; no
+    # measured FP32 peak exists)
+    fp32_peak = 148 * 128 * 2 * (clocks.get("sm_mhz") or 1965.0) * 1e6 / 1e12
+    rooflines = {
+        "transpose_statistics": {"bound": "hbm", "achieved": kern["transpose_statistics"]["gbs"],
+                                 "peak": hbm_peak, "unit": "GB/s",
+                                 "frac": kern["transpose_statistics"]["gbs"] / hbm_peak},
+        "incoherent_beamformer": {"bound": "hbm", "achieved": kern["incoherent_beamformer"]["gbs"],
+                                  "peak": hbm_peak, "unit": "GB/s",
+                                  "frac": kern["incoherent_beamformer"]["gbs"] / hbm_peak},
+        "coherent_dedispersion": {"bound": "fp32 (CUDA cores); measured limit: shared-memory pipe",
+                                  "achieved": kern["coherent_dedispersion"]["gflops"] / 1e3,
+                                  "peak": fp32_peak, "unit": "TFLOP/s",
+                                  "frac": kern["coherent_dedispersion"]["gflops"] / 1e3 / fp32_peak,
+                                  "peak_source": "nominal at the median SM clock"}}
     ops_gulp = 8.0 * A * B * 2 * F * T * len(dms)
     # weights, history copy, transpose + statistics and its finalize, IB channel
     # order, CDD, IB per DM, CB
@@ -502,7 +519,8 @@ def main_b200(args):
             "cb_int8_tops": cb["tops"],
             "plain": {"value": gulp_s / (ms_plain * 1e-3) * world, "ms_per_step": ms_plain},
             "batched_vs_plain": ms_plain / ms_graph, "ragged": ragged,
-            "kernels": kern, "roofline": roof, "hbm_peak_gbs": hbm_peak, "e2e": e2e,
+            "kernels": kern, "roofline": roof, "rooflines": rooflines, "hbm_peak_gbs": hbm_peak,
+            "e2e": e2e,
             "cdd_plan": plan_dev,
             "autotune": {k: tune[k] for k in ("fft_len", "cb_tiles_per_item", "cb_voltage_stages",
                                               "cb_weight_stages")},
@@ -1020,7 +1038,8 @@ def profile_case(which, nchans=16, reps=3):
     warm-up launch and `reps` profiled launches of one kernel.  `idd`: the
     UHF incoherent-dedispersion trials (128 DMs over 0-100, 256 channels,
     2048 beams) on 4096 output samples, a 5.9 GB beam buffer.  `bw`: the
-    transpose, statistics and incoherent-beam kernels on the same channels.""" 
+    transpose, statistics, fused transpose + statistics and incoherent-beam
+    kernels on the same channels.""" 
     import torch
 
     from skyweaver_b200 import stages, synthetic
@@ -1061,6 +1080,7 @@ def profile_case(which, nchans=16, reps=3):
         for _ in range(1 + reps):
             stages.transpose_fpact(taftp, A, out=fpact)
             stages.statistics(fpact, T)
+            stages.transpose_fpact_statistics(taftp, A, out=fpact)  # the pipeline's form
             stages.incoherent_beamform(fpact, T, ts, scl, scl, bw)
         torch.cuda.synchronize()
         print(f"profile case bw: {nchans} channels, {1 + reps} launches of each stage ok")
