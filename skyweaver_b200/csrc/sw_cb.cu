@@ -54,6 +54,7 @@ constexpr int kMaxProblems = 96;
 // once per 32 samples instead of once per 16: measured 2.6 % faster than
 // 16 warps sharing every tile).
 constexpr int kEpiWarps    = 16;
+static_assert(kEpiWarps == 8 || kEpiWarps == 16, "one or two epilogue warps per TMEM lane quarter");
 constexpr int kThreads     = 32 * (2 + kEpiWarps);
 constexpr int kTmemCols    = 512;
 
@@ -537,15 +538,16 @@ cb_kernel(const __grid_constant__ Params P)
         }
     } else {
         // ------------------------------------------------------ epilogue
-        constexpr int kSlice  = 32;                  // samples per warp per tile
+        constexpr int kHalves = kEpiWarps / 8;       // warps per TMEM lane quarter and group
+        constexpr int kSlice  = kTileT / kHalves;    // samples per warp per tile
         // TMEM columns per load group: 16 (measured 1.5 % faster than 8),
         // except for full Stokes at tscrunch <= 4, whose many outputs per
         // group leave too few registers for it
         constexpr int kG      = (STOKES == 4 && TS <= 4) ? 8 : 16;
         constexpr int kGroups = kSlice / kG;         // column groups per warp
         const int q   = warp & 3;               // TMEM lane quarter of this warp
-        const int h   = ((warp - 2) >> 2) & 1;  // which half of the tile's 64 samples
-        const int grp = (warp - 2) >> 3;        // accumulator buffer this warp drains
+        const int h   = ((warp - 2) >> 2) % kHalves;  // which part of the tile's samples
+        const int grp = (warp - 2) / (kEpiWarps / 2); // accumulator buffer this warp drains
         const int F = P.nchans;
         const int nout = P.nsamples / TS;
         const uint32_t lane_base = tmem + ((uint32_t)(q * 32) << 16);
@@ -601,7 +603,7 @@ cb_kernel(const __grid_constant__ Params P)
                 }
                 if(!mbar_wait(acc_full_s + 8 * grp, aph, s_abort, deadline, P.err)) { ok = false; break; }
                 // the tile's MMAs are complete, so its voltage stage is free
-                if(warp == 2 + 8 * grp && lane == 0)
+                if(warp == 2 + (kEpiWarps / 2) * grp && lane == 0)
                     mbar_arrive(&v_empty[(seq + tile - tile0) % nvs]);
                 fence_after();
                 float power[NC];  // carried across groups while tscrunch > 8
