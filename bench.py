@@ -464,9 +464,30 @@ def main_b200(args):
     ms_e2e = time_steps(lambda i: pipe.process_host(h_ins[i % PULSE_EVERY == 10],
                                                     epoch0 + i * gulp_s, h_out),
                         k_e2e, args.warmup)
+    # the transfer bound: the same bytes copied both ways at once (pinned host
+    # buffers, one stream per direction), with no compute
+    d_out_copy = torch.empty(cb_bytes, dtype=torch.int8, device="cuda")
+    d_in_copy = torch.empty(h_in.numel(), dtype=torch.int8, device="cuda")
+    s_up, s_dn = torch.cuda.Stream(), torch.cuda.Stream()
+
+    def both_ways():
+        with torch.cuda.stream(s_up):
+            d_in_copy.copy_(h_in, non_blocking=True)
+        with torch.cuda.stream(s_dn):
+            h_out.copy_(d_out_copy, non_blocking=True)
+
+    both_ways()
+    torch.cuda.synchronize()
+    t_copy = time.perf_counter()
+    for _ in range(5):
+        both_ways()
+    torch.cuda.synchronize()
+    ms_copy = (time.perf_counter() - t_copy) / 5 * 1e3
+    del d_out_copy, d_in_copy
     e2e = {"value": gulp_s / (ms_e2e * 1e-3) * world, "unit": "x real-time",
            "h2d_bytes_per_step": int(h_in.numel()), "d2h_bytes_per_step": int(cb_bytes),
-           "ms_per_step": ms_e2e, "steps": k_e2e}
+           "ms_per_step": ms_e2e, "steps": k_e2e,
+           "transfer_bound_ms": ms_copy, "frac_of_transfer_bound": ms_copy / ms_e2e}
 
     peaks = {}
     pk = os.path.join(REPO, "MEASURED_PEAKS.json")
