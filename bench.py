@@ -467,7 +467,7 @@ def main_b200(args):
     # the transfer bound: the same bytes copied both ways at once (pinned host
     # buffers, one stream per direction), with no compute
     d_out_copy = torch.empty(cb_bytes, dtype=torch.int8, device="cuda")
-    d_in_copy = torch.empty(h_in.numel(), dtype=torch.int8, device="cuda")
+    d_in_copy = torch.empty(h_in.shape, dtype=torch.int8, device="cuda")
     s_up, s_dn = torch.cuda.Stream(), torch.cuda.Stream()
 
     def both_ways():
