@@ -1015,21 +1015,32 @@ def uhf_case(torch, stages, synthetic, K, W, pulses=True):
     taftp = taftp.round_().clamp_(-127, 127).to(torch.int8)
     stream = torch.cuda.current_stream()
 
-    def gulp(i):
+    def gulp(i, mark=None):
         pipe.process_device(taftp, 1.7e9 + i * T / chbw)
+        if mark is not None:  # end of the beamforming pipeline's part
+            mark.record(stream)
         for d in range(len(blocks)):
             idp.push(d, pipe.cb_device(d))
 
     for i in range(W):
         gulp(i)
     torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+    e0, e1 = ev(), ev()
+    starts, mids = [ev() for _ in range(K)], [ev() for _ in range(K)]
     e0.record(stream)
     for i in range(K):
-        gulp(W + i)
+        starts[i].record(stream)
+        gulp(W + i, mids[i])
     e1.record(stream)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / K
+    # per gulp: the beamforming pipeline, then the incoherent-dedispersion
+    # pipeline (pushes into its aggregation buffers and, every dispatch
+    # samples, the dedispersion and its overlap copy)
+    ends = starts[1:] + [e1]
+    ms_bf = sum(a.elapsed_time(b) for a, b in zip(starts, mids)) / K
+    ms_idd = sum(b.elapsed_time(c) for b, c in zip(mids, ends)) / K
     geo = [idp.geometry(b) for b in range(len(blocks))]
     idp.close()
     del taftp
@@ -1042,7 +1053,9 @@ def uhf_case(torch, stages, synthetic, K, W, pulses=True):
                        "with RFI tones at 20 sigma in channels 40, 130 and 200",
            "ms_per_gulp": ms, "rtf": gulp_s / (ms * 1e-3),
            "idd_adds_per_gulp": adds, "idd_overlap_samples": [g[1] for g in geo],
-           "cdd_plan": list(pipe.cdd_plan()), "timed_gulps": K, "warmup_gulps": W}
+           "cdd_plan": list(pipe.cdd_plan()), "timed_gulps": K, "warmup_gulps": W,
+           "ms_per_gulp_split": {"beamforming_pipeline": ms_bf,
+                                 "incoherent_dedispersion_pipeline": ms_idd}}
     if pulses:
         _, lag = pipe.cdd_plan()[1:]
         dl, _, sf = blocks[1]
