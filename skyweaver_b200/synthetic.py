@@ -4,7 +4,7 @@ shapes, sizes and value distributions).
 
 * voltages: complex Gaussian, sigma per component (default 8), rounded and
   clipped to [-127, 127], TAFTP order [heap][antenna][channel][256][pol][re,im]
-* optional dispersed pulse and narrowband RFI tones
+* narrowband RFI tones; dispersed bursts (BurstInjector, on the device)
 * delay models: antenna positions uniform in a disk of `array_radius` metres,
   beam directions uniform within `fov_deg` of boresight,
   tau_ab = (x_a l_b + y_a m_b) / c, stored as float3 (weight, offset, rate)
@@ -32,23 +32,6 @@ def channel_frequencies(centre: float, bandwidth: float, nchans: int) -> np.ndar
     """PipelineConfig::calculate_channel_frequencies (PipelineConfig.cpp:188-203)."""
     chbw = bandwidth / nchans
     return centre - bandwidth / 2.0 + chbw / 2.0 + chbw * np.arange(nchans)
-
-
-def inject_pulse(taftp: np.ndarray, freqs: np.ndarray, tsamp: float, dm: float,
-                 t0: int, width: int, amplitude: float, g: np.random.Generator) -> None:
-    """Add a dispersed broadband pulse (arrival referenced to the top channel)
-    in place: extra complex Gaussian power of `amplitude` sigma-units."""
-    nheaps, nant, nchans = taftp.shape[:3]
-    fref = freqs.max()
-    for c, f in enumerate(freqs):
-        delay = int(round(DM_CONST * dm * (1 / f ** 2 - 1 / fref ** 2) / tsamp))
-        start = t0 + delay
-        for t in range(start, start + width):
-            h, s = divmod(t, 256)
-            if 0 <= h < nheaps:
-                extra = g.normal(0, amplitude, size=(nant, 2, 2))
-                cur = taftp[h, :, c, s].astype(np.float32) + extra
-                taftp[h, :, c, s] = np.clip(np.rint(cur), -127, 127).astype(np.int8)
 
 
 def inject_tones(taftp: np.ndarray, channels, amplitude: float) -> None:

@@ -48,6 +48,8 @@ def test_transpose_fpact_matches_ftpa(cuda, oracle):
     assert np.array_equal(got, ref.transpose(0, 2, 3, 4, 1))
     back = _np(stages.fpact_to_ftpa(fp, 1024, offset=32))
     assert np.array_equal(back, ref)
+    fp2 = _np(stages.ftpa_to_fpact(_dev(cuda, ref), row_stride=1024 + 32, offset=32))
+    assert np.array_equal(fp2[..., 32:], got)
 
 
 def test_keep_history(cuda):
@@ -79,7 +81,7 @@ def test_statistics(cuda, oracle):
 def test_transpose_statistics_fused_equals_separate(cuda, oracle, nheaps, in_nant, out_nant):
     """The one-pass transpose + statistics writes the same FPACT bytes and the
     same statistics (bit for bit) as the two separate stages, padded
-    antennas and a heap count that is not a multiple of the CTA's 16 heaps
+    antennas and a heap count that is not a multiple of the CTA's 8 heaps
     included; the statistics match the oracle within its tolerance."""
     from skyweaver_b200 import stages, synthetic
     g = synthetic.rng(4242)
