@@ -75,6 +75,8 @@ _SIGS = {
     "sw_fpact_to_ftpa": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_size_t,
                                  c_size_t, c_void_p]),
     "sw_fpact_keep_history": (c_int, [c_void_p, c_size_t, c_size_t, c_size_t, c_void_p]),
+    "sw_fpact_copy_history": (c_int, [c_void_p, c_void_p, c_size_t, c_size_t, c_size_t,
+                                      c_void_p]),
     "sw_statistics_scratch_bytes": (c_size_t, [c_int, c_int, c_int]),
     "sw_statistics": (c_int, [c_void_p, c_size_t, c_size_t, c_int, c_int, c_int, c_int,
                               c_void_p, c_void_p, c_void_p]),

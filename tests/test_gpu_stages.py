@@ -65,6 +65,26 @@ def test_keep_history(cuda):
     assert np.array_equal(got[:, hist:], a[:, hist:])
 
 
+def test_copy_history_between_row_sets(cuda):
+    """sw_fpact_copy_history: the last `hist` samples of every row of one row
+    set land at the front of the same row of the other; the source rows and
+    the rest of the destination rows are untouched (the pipeline alternates
+    two row sets this way)."""
+    from skyweaver_b200._lib import call
+    import ctypes
+    rows, hist, T = 7, 48, 160
+    g = np.random.default_rng(3)
+    a = g.integers(-128, 128, size=(rows, hist + T), dtype=np.int8)
+    b = g.integers(-128, 128, size=(rows, hist + T), dtype=np.int8)
+    da, db = _dev(cuda, a), _dev(cuda, b)
+    call("sw_fpact_copy_history", ctypes.c_void_p(da.data_ptr()), ctypes.c_void_p(db.data_ptr()),
+         rows, hist + T, hist, ctypes.c_void_p(cuda.cuda.current_stream().cuda_stream))
+    ga, gb = _np(da), _np(db)
+    assert np.array_equal(ga, a)
+    assert np.array_equal(gb[:, :hist], a[:, T:T + hist])
+    assert np.array_equal(gb[:, hist:], b[:, hist:])
+
+
 # ------------------------------------------------------------ statistics
 def test_statistics(cuda, oracle):
     from skyweaver_b200 import stages, synthetic
