@@ -314,6 +314,16 @@ def test_coherent_beam_stokes(cuda, oracle, stokes, ib_sub):
     assert np.array_equal(out, out2), _report(out2, out)
 
 
+@pytest.mark.parametrize("ts", [1, 2, 8])
+@pytest.mark.parametrize("stokes", ["I", "Q", "U"])
+def test_coherent_beam_short_tscrunch(cuda, oracle, ts, stokes):
+    """tscrunch 1, 2 and 8 (bit-exact like 4, 16 and 32 above)."""
+    out, ref, dbg, volts = _cb_case(cuda, oracle, 64, 256, 3, 2, ts, stokes, stokes == "I",
+                                    seed=24)
+    assert np.array_equal(dbg, volts)
+    assert np.array_equal(out, ref), _report(out, ref)
+
+
 def test_coherent_beam_partial_block_and_tscrunch(cuda, oracle):
     out, ref, _, _ = _cb_case(cuda, oracle, 64, 96, 2, 1, 32, "I", True, seed=23)
     assert np.array_equal(out, ref)
