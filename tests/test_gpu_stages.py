@@ -97,7 +97,8 @@ def test_statistics(cuda, oracle):
     np.testing.assert_allclose(got, ref, rtol=1e-5, atol=1e-6)
 
 
-@pytest.mark.parametrize("nheaps,in_nant,out_nant", [(8, 64, 64), (20, 57, 64), (3, 12, 16)])
+@pytest.mark.parametrize("nheaps,in_nant,out_nant", [(8, 64, 64), (20, 57, 64), (3, 12, 16),
+                                                    (5, 9, 18)])
 def test_transpose_statistics_fused_equals_separate(cuda, oracle, nheaps, in_nant, out_nant):
     """The one-pass transpose + statistics writes the same FPACT bytes and the
     same statistics (bit for bit) as the two separate stages, padded
