@@ -325,8 +325,13 @@ def test_coherent_beam_short_tscrunch(cuda, oracle, ts, stokes):
     assert np.array_equal(out, ref), _report(out, ref)
 
 
-def test_coherent_beam_partial_block_and_tscrunch(cuda, oracle):
-    out, ref, _, _ = _cb_case(cuda, oracle, 64, 96, 2, 1, 32, "I", True, seed=23)
+@pytest.mark.parametrize("A", [16, 32, 64])
+def test_coherent_beam_partial_block_and_tscrunch(cuda, oracle, A):
+    """96 beams (a partial 128-beam block), tscrunch 32, and every supported
+    antenna count: K = 2 A bytes = 1, 2 or 4 MMA K steps with the SW32, SW64 or
+    SW128 weight layouts."""
+    out, ref, dbg, volts = _cb_case(cuda, oracle, A, 96, 2, 1, 32, "I", True, seed=23)
+    assert np.array_equal(dbg, volts)
     assert np.array_equal(out, ref)
 
 
