@@ -516,6 +516,34 @@ def test_incoherent_dedispersion_many_channels(cuda, oracle, fill):
         assert np.all(ref == int(fill * F * ts / 1000.0))
 
 
+@pytest.mark.parametrize("F,B,ndms,ts,misalign", [
+    (8, 1040, 37, 1, 0),   # 16-beam path: 65 lanes -> beam blocks of 32, 32, 1; DM groups 16, 16, 5
+    (16, 528, 3, 5, 0),    # 16-beam path: 33 lanes -> two beam blocks, one DM group
+    (12, 20, 5, 3, 0),     # 4-beam path: 5 beam quads
+    (16, 64, 18, 2, 4),    # beams a multiple of 16 but the TFB only 4-byte aligned -> 4-beam path
+])
+def test_incoherent_dedispersion_launch_shapes(cuda, oracle, F, B, ndms, ts, misalign):
+    """Beam counts and DM counts that leave partial beam blocks and partial DM
+    groups in the launch grid, and a TFB that does not start on a 16-byte
+    boundary: every output must still equal the oracle's."""
+    from skyweaver_b200 import stages, synthetic
+    g = synthetic.rng(1000 + B + ndms)
+    freqs = synthetic.channel_frequencies(1284e6, F * 856e6 / 1024, F)
+    dms = np.linspace(0.0, 60.0, ndms).astype(np.float32)
+    delays, maxd = oracle.idd_delays(freqs, dms, 16 / (856e6 / 1024))
+    T = maxd + 40 * ts
+    tfb = g.integers(-128, 128, size=(T, F, B), dtype=np.int8)
+    sf = np.float32(math.sqrt(F * ts))
+    ref = oracle.idd(tfb, delays, maxd, ts, sf)
+    buf = cuda.empty(tfb.size + 16, dtype=cuda.int8, device="cuda")
+    d_tfb = buf[misalign:misalign + tfb.size].view(T, F, B)
+    d_tfb.copy_(cuda.from_numpy(tfb))
+    assert d_tfb.data_ptr() % 16 == misalign
+    got = _np(stages.incoherent_dedisperse(d_tfb, _dev(cuda, delays), maxd, ts, float(sf)))
+    assert got.shape == (40, ndms, B)
+    assert np.array_equal(got, ref)
+
+
 def test_incoherent_dedispersion_ones(cuda, oracle):
     """IncoherentDedisperserTester.cu:96-126: all-ones input -> sqrt(F*ts)."""
     from skyweaver_b200 import stages, synthetic
