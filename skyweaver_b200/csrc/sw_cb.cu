@@ -545,6 +545,12 @@ cb_kernel(const __grid_constant__ Params P)
         // group leave too few registers for it
         constexpr int kG      = (STOKES == 4 && TS <= 4) ? 8 : 16;
         constexpr int kGroups = kSlice / kG;         // column groups per warp
+        // Release the accumulator buffer as soon as the tile's last column
+        // group is in registers, before its arithmetic, when several outputs
+        // per group follow the last load (tscrunch <= 8: measured 3.4 %
+        // faster at tscrunch 8); at tscrunch 16 the release after the
+        // arithmetic measured 0.9 % faster.
+        constexpr bool kEarlyRelease = TS <= 8;
         const int q   = warp & 3;               // TMEM lane quarter of this warp
         const int h   = ((warp - 2) >> 2) % kHalves;  // which part of the tile's samples
         const int grp = (warp - 2) / (kEpiWarps / 2); // accumulator buffer this warp drains
@@ -629,6 +635,11 @@ cb_kernel(const __grid_constant__ Params P)
                         SW_TMEM_LD8(ta + 192, i1);
                     }
                     tmem_wait_ld();
+                    if(kEarlyRelease && g == kGroups - 1) {
+                        fence_before();
+                        __syncwarp();
+                        if(lane == 0) mbar_arrive(&acc_empty[grp]);
+                    }
                     const int tbase = tile * kTileT + h * kSlice + g * kG;
                     if(DBG && valid) {
                         int2* dbg = reinterpret_cast<int2*>(P.debug);
@@ -689,9 +700,11 @@ cb_kernel(const __grid_constant__ Params P)
                         }
                     }
                 }
-                fence_before();
-                __syncwarp();
-                if(lane == 0) mbar_arrive(&acc_empty[grp]);
+                if(!kEarlyRelease) {
+                    fence_before();
+                    __syncwarp();
+                    if(lane == 0) mbar_arrive(&acc_empty[grp]);
+                }
                 aph ^= 1;
                 outp += (2 * kTileT / TS) * out_emit;
                 if(P.ib_subtract) ibq += (2 * kTileT / TS) * ib_emit;
