@@ -112,6 +112,33 @@ def test_delay_file_fixture_layout():
     assert sets.nbeamsets == 2
 
 
+def test_delay_manager_epochs_and_beamsets():
+    """DelayManagerTester.cu:54-92 on the same file: reads in the first and the
+    nth validity window give nbeams x nantennas delays (padded with zeros
+    past the model's 67 beams x 57 antennas), an epoch before the first
+    window raises InvalidDelayEpoch, one after the last window raises
+    RuntimeError, and the file holds 2 beamsets."""
+    from skyweaver_b200 import delays
+    path = os.path.join(GOLDEN, "test_delays.bin")
+    models = delays.read_delay_file(path)
+    dm = delays.DelayManager(path, nbeams=96, nantennas=64)
+    first = dm.delays(1708082169.0)
+    assert first.shape == (96, 64, 3)
+    assert np.array_equal(first[:67, :57], models[0].delays)
+    assert not first[67:].any() and not first[:, 57:].any()
+    nth = dm.delays(1708082409.957)
+    k = next(i for i, m in enumerate(models) if m.start_epoch <= 1708082409.957 <= m.end_epoch)
+    assert k > 0 and np.array_equal(nth[:67, :57], models[k].delays)
+    assert abs(models[-1].end_epoch - 1708082468.957) < 1e-3
+    assert dm.nbeamsets() == 2
+    with pytest.raises(delays.InvalidDelayEpoch):
+        delays.DelayManager(path, nbeams=96, nantennas=64).delays(1708082165.0)
+    with pytest.raises(RuntimeError):
+        delays.DelayManager(path, nbeams=96, nantennas=64).delays(1708082470.957)
+    with pytest.raises(RuntimeError, match="too many beams"):
+        delays.DelayManager(path, nbeams=64, nantennas=64)
+
+
 def _declared_functions():
     with open(os.path.join(REPO, "include", "skyweaver_b200.h")) as f:
         txt = f.read()
