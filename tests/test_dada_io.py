@@ -108,3 +108,22 @@ def test_output_paths_follow_multifilewriter():
     assert d == "/data/2024-02-16-11:17:09/3/1284000000"
     assert base == "sw_2024-02-16-11:17:09_3_00150.000_1284000000_cb"
     assert ext == ".tdb"
+
+
+def test_reader_eof_zero_size_and_missing_file(tmp_path):
+    """MultiFileReaderTester.cu:97-130: seeking to the payload's end is legal
+    and leaves nothing to read, one byte past it raises, a read of 0 bytes
+    returns 0, and a file that does not exist raises when the reader opens."""
+    from skyweaver_b200 import dada
+    payload = np.arange(3000, dtype=np.int64).astype(np.int8)
+    r = dada.MultiFileReader(_write_files(tmp_path, payload, [1000, 2000]))
+    r.seek(r.total_bytes())
+    assert r.tell() == r.total_bytes() == 3000
+    assert len(r.read(10)) == 0
+    with pytest.raises(Exception, match="Invalid seek position"):
+        r.seek(r.total_bytes() + 1)
+    r.seek(0)
+    assert len(r.read(0)) == 0 and r.tell() == 0
+    r.close()
+    with pytest.raises(Exception, match="Could not open file"):
+        dada.MultiFileReader([str(tmp_path / "non_existent_file.dada")])
