@@ -329,6 +329,7 @@ class IncoherentDedispersionPipeline:
 
     def __init__(self, nchans, nbeams, blocks, handler, dispatch=None):
         self.handler = handler
+        self.nchans, self.nbeams = int(nchans), int(nbeams)
         nb = len(blocks)
         self._delays = [np.ascontiguousarray(b[0], np.int32) for b in blocks]
         ndms = (ctypes.c_int * nb)(*[d.shape[0] for d in self._delays])
@@ -349,7 +350,15 @@ class IncoherentDedispersionPipeline:
         self.handler(block, tdb.reshape(nout, ndms, nbeams))
 
     def push(self, block, tfb, stream=None):
-        call("sw_idd_pipeline_push", self.h, block, _ptr(tfb), tfb.shape[0], _stream(stream))
+        """Append whole time samples: like AggregationBuffer::push_back
+        (AggregationBuffer.cu:53-56), a length that is not a multiple of one
+        sample (nchans x nbeams bytes) raises RuntimeError."""
+        row = self.nchans * self.nbeams
+        n = tfb.numel()
+        if tfb.dtype != torch.int8 or not tfb.is_contiguous() or n % row:
+            raise RuntimeError(f"input size is not a multiple of the slot size ({n} int8 values, "
+                               f"slots of {self.nchans} x {self.nbeams})")
+        call("sw_idd_pipeline_push", self.h, block, _ptr(tfb), n // row, _stream(stream))
 
     def geometry(self, block):
         v = [ctypes.c_int() for _ in range(4)]

@@ -580,6 +580,51 @@ def test_incoherent_dedispersion_char4_iquv(cuda, oracle):
         assert np.array_equal(got[..., c], ref)
 
 
+def test_incoherent_dedispersion_pipeline_push_semantics(cuda, oracle):
+    """AggregationBufferTester.cu:30-109 through the device pipeline. With one
+    channel, one DM of delay 0, tscrunch 1 and scale 1 the dedisperser is the
+    identity, so each dispatch hands back the buffer itself: one push of one
+    dispatch (10 samples of 4 beams) fires one dispatch equal to it; a push
+    of 100 samples fires 10, the last holding samples 90..99. With an overlap
+    (two channels, delays {1, 0}: overlap 1) a 100-sample push fires
+    (100 - 1) // 10 = 9 dispatches, the k-th covering samples
+    [10 k, 10 k + 11). A push that is not whole samples raises."""
+    from skyweaver_b200 import stages, synthetic
+    g = synthetic.rng(47)
+    B = 4
+    got = []
+    ident = [(np.zeros((1, 1), np.int32), 1, 1.0)]
+    pipe = stages.IncoherentDedispersionPipeline(1, B, ident, lambda b, t: got.append(_np(t)),
+                                                 dispatch=[10])
+    one = g.integers(-128, 128, size=(10, 1, B), dtype=np.int8)
+    pipe.push(0, _dev(cuda, one))
+    cuda.cuda.synchronize()
+    assert len(got) == 1 and np.array_equal(got[0][:, 0, :], one[:, 0, :])
+    got.clear()
+    many = g.integers(-128, 128, size=(100, 1, B), dtype=np.int8)
+    pipe.push(0, _dev(cuda, many))
+    cuda.cuda.synchronize()
+    assert len(got) == 10 and np.array_equal(got[-1][:, 0, :], many[90:, 0, :])
+    with pytest.raises(RuntimeError, match="slot size"):
+        pipe.push(0, _dev(cuda, g.integers(-128, 128, size=101, dtype=np.int8)))
+    pipe.close()
+
+    got = []
+    delays = np.array([[1, 0]], np.int32)
+    pipe = stages.IncoherentDedispersionPipeline(2, B, [(delays, 1, 1.0)],
+                                                 lambda b, t: got.append(_np(t)), dispatch=[10])
+    assert pipe.geometry(0) == (10, 1, 10, 1)
+    data = g.integers(-128, 128, size=(100, 2, B), dtype=np.int8)
+    pipe.push(0, _dev(cuda, data))
+    cuda.cuda.synchronize()
+    pipe.close()
+    assert len(got) == 9
+    for k, tdb in enumerate(got):
+        ref = oracle.idd(np.ascontiguousarray(data[10 * k:10 * k + 11]), delays, 1, 1,
+                         np.float32(1.0))
+        assert np.array_equal(tdb, ref), k
+
+
 def test_incoherent_dedispersion_pipeline_aggregation(cuda, oracle):
     """Device AggregationBuffer semantics (AggregationBuffer.cu:23-117): with
     dispatch D and overlap O = max delay, dispatch k covers samples
