@@ -1073,10 +1073,16 @@ def profile_case(which, nchans=16, reps=3):
     UHF incoherent-dedispersion trials (128 DMs over 0-100, 256 channels,
     2048 beams) on 4096 output samples, a 5.9 GB beam buffer.  `bw`: the
     transpose, statistics, fused transpose + statistics and incoherent-beam
-    kernels on the same channels.""" 
+    kernels on the same channels.  `uhf`: the UHF leg's chain (C4) without
+    its burst stream, 4 warm-up + 4 timed gulps, for the launch list (one-pass
+    `gpu__time_duration.sum` only: it holds tens of GB)."""
     import torch
 
     from skyweaver_b200 import stages, synthetic
+    if which == "uhf":
+        r = uhf_case(torch, stages, synthetic, 4, 4, pulses=False)
+        print(json.dumps({"profile case uhf": r}))
+        return
     if which == "idd":
         U = UHF
         F, B, D = U["nchans"], U["nbeams"], 4096
@@ -1149,7 +1155,7 @@ def profile_case(which, nchans=16, reps=3):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--profile", choices=["cb", "cdd", "idd", "bw"], default=None,
+    ap.add_argument("--profile", choices=["cb", "cdd", "idd", "bw", "uhf"], default=None,
                     help="run a small single-kernel case for ncu and exit")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
