@@ -97,6 +97,31 @@ def test_statistics(cuda, oracle):
     np.testing.assert_allclose(got, ref, rtol=1e-5, atol=1e-6)
 
 
+@pytest.mark.parametrize("fill", ["zeros", "constant", "two_values"])
+def test_statistics_degenerate_inputs(cuda, oracle, fill):
+    """StatisticsCalculatorTester.cu:195-205 runs the statistics on a
+    zero-initialised gulp. Zero and constant series have no variance, so
+    skewness and kurtosis are 0/0 = NaN in the reference's formulas
+    (StatisticsCalculator.cu:80-83), and must be NaN here too; a series of
+    two values has exact moments."""
+    from skyweaver_b200 import stages
+    T, A, F = 1024, 8, 3
+    taftp = np.zeros((T // 256, A, F, 256, 2, 2), np.int8)
+    if fill == "constant":
+        taftp[:] = -7
+    elif fill == "two_values":
+        taftp[..., 0] = 3
+        taftp[..., 1] = -5
+    ref = oracle.statistics(oracle.transpose(taftp, A))
+    got = _np(stages.statistics(stages.transpose_fpact(_dev(cuda, taftp), A), T))
+    np.testing.assert_allclose(got, ref, rtol=1e-5, atol=1e-6, equal_nan=True)
+    if fill != "two_values":
+        assert np.isnan(got[..., 2:]).all() and not np.isnan(got[..., :2]).any()
+    else:
+        assert np.allclose(got[..., 0], -1.0) and np.allclose(got[..., 1], 4.0 * math.sqrt(
+            2 * T / (2 * T - 1)), rtol=1e-6)
+
+
 @pytest.mark.parametrize("nheaps,in_nant,out_nant", [(8, 64, 64), (20, 57, 64), (3, 12, 16),
                                                     (5, 9, 18)])
 def test_transpose_statistics_fused_equals_separate(cuda, oracle, nheaps, in_nant, out_nant):
