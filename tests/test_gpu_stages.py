@@ -341,9 +341,11 @@ def test_coherent_beam_stokes(cuda, oracle, stokes, ib_sub):
 
 
 @pytest.mark.parametrize("ts", [1, 2, 8])
-@pytest.mark.parametrize("stokes", ["I", "Q", "U"])
+@pytest.mark.parametrize("stokes", ["I", "Q", "U", "V", "IQUV"])
 def test_coherent_beam_short_tscrunch(cuda, oracle, ts, stokes):
-    """tscrunch 1, 2 and 8 (bit-exact like 4, 16 and 32 above)."""
+    """tscrunch 1, 2 and 8 (bit-exact like 4, 16 and 32 above), where the
+    epilogue hands its accumulator buffer back before the last column
+    group's arithmetic; full Stokes at tscrunch <= 4 reads 8-column groups."""
     out, ref, dbg, volts = _cb_case(cuda, oracle, 64, 256, 3, 2, ts, stokes, stokes == "I",
                                     seed=24)
     assert np.array_equal(dbg, volts)
