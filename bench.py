@@ -1069,9 +1069,10 @@ def uhf_case(torch, stages, synthetic, K, W, pulses=True):
 def profile_case(which, nchans=16, reps=3):
     """Small single-kernel case for ncu captures: `nchans` channels of the
     benchmark workload (268 MB of voltages for 16 channels, above L2), one
-    warm-up launch and `reps` profiled launches of one kernel.  `idd`: the
-    UHF incoherent-dedispersion trials (128 DMs over 0-100, 256 channels,
-    2048 beams) on 4096 output samples, a 5.9 GB beam buffer.  `bw`: the
+    warm-up launch and `reps` profiled launches of one kernel.  `cb8`: the
+    `cb` case at tscrunch 8.  `idd`: the UHF incoherent-dedispersion trials
+    (128 DMs over 0-100, 256 channels) for 1024 of the 2048 beams on 4096
+    output samples, a 2.9 GB beam buffer.  `bw`: the
     transpose, statistics, fused transpose + statistics and incoherent-beam
     kernels on the same channels.  `uhf`: the UHF leg's chain (C4) without
     its burst stream, 4 warm-up + 4 timed gulps, for the launch list (one-pass
@@ -1085,7 +1086,7 @@ def profile_case(which, nchans=16, reps=3):
         return
     if which == "idd":
         U = UHF
-        F, B, D = U["nchans"], U["nbeams"], 4096
+        F, B, D = U["nchans"], U["nbeams"] // 2, 4096   # 2.9 GB of beams
         freqs = U["top"] - F * U["chbw"] + U["chbw"] * (np.arange(F) + 0.5)
         cb_tsamp = U["tscrunch"] / U["chbw"]
         trials = np.linspace(0.0, 2 * U["trial_span"], U["ntrials"]).astype(np.float32)
@@ -1127,7 +1128,8 @@ def profile_case(which, nchans=16, reps=3):
         return
     fp = (torch.randn((F, 2, A, 2, T), generator=gen, device="cuda") * 8).round_().clamp_(-127, 127)
     fp = fp.to(torch.int8)
-    if which == "cb":
+    if which in ("cb", "cb8"):
+        ts = 8 if which == "cb8" else ts
         g = synthetic.rng(3)
         freqs = stages.channel_frequencies(WORK["centre"], F * WORK["chbw"], F)
         _, gemm = stages.generate_weights(dev(synthetic.delay_model(g, B, A)), dev(freqs),
@@ -1155,7 +1157,7 @@ def profile_case(which, nchans=16, reps=3):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--profile", choices=["cb", "cdd", "idd", "bw", "uhf"], default=None,
+    ap.add_argument("--profile", choices=["cb", "cb8", "cdd", "idd", "bw", "uhf"], default=None,
                     help="run a small single-kernel case for ncu and exit")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
